@@ -1,0 +1,227 @@
+// aes.cuh -- AES-128 in the counter mode the reference uses for P1||P2 expansion
+// (reference src/aes128_ctr.cu:124-283): key = seed_pk, block i encrypts the 16-byte counter
+// 0^8 || BE64(i), output bytes in standard AES order, a final partial block keeps its leading
+// bytes.
+//
+// B200 layout: one round table T0 (Te0 of FIPS-197 in big-endian words) replicated 32 times in
+// shared memory, entry x of copy c at word 32*x + c, so lane c always hits bank c and the 16
+// data-dependent lookups of a round never conflict.  The other three tables are byte rotations
+// of T0 (PRMT).  The S-box for the last round is byte 1 of T0[x].  Tables are computed at compile
+// time from GF(2^8) arithmetic.
+#pragma once
+
+#include "common.cuh"
+
+namespace mayo {
+
+struct AesTables {
+    uint32_t te0[256];
+    uint8_t sbox[256];
+};
+
+__host__ __device__ constexpr uint8_t gf256_mulc(uint8_t a, uint8_t b) {
+    uint8_t r = 0;
+    for (int i = 0; i < 8; i++) {
+        if (b & 1) r ^= a;
+        uint8_t hi = a & 0x80;
+        a = (uint8_t)(a << 1);
+        if (hi) a ^= 0x1B;
+        b >>= 1;
+    }
+    return r;
+}
+
+__host__ __device__ constexpr AesTables make_aes_tables() {
+    AesTables t{};
+    // exp/log over the generator 0x03
+    uint8_t ex[256] = {}, lg[256] = {};
+    uint8_t g = 1;
+    for (int i = 0; i < 255; i++) {
+        ex[i] = g;
+        lg[g] = (uint8_t)i;
+        g = gf256_mulc(g, 3);
+    }
+    for (int x = 0; x < 256; x++) {
+        uint8_t inv = x ? ex[(255 - lg[x]) % 255] : 0;
+        uint8_t s = inv, r = inv;
+        for (int i = 0; i < 4; i++) {
+            r = (uint8_t)((r << 1) | (r >> 7));
+            s ^= r;
+        }
+        s ^= 0x63;
+        t.sbox[x] = s;
+        t.te0[x] = ((uint32_t)gf256_mulc(s, 2) << 24) | ((uint32_t)s << 16) | ((uint32_t)s << 8) |
+                   (uint32_t)gf256_mulc(s, 3);
+    }
+    return t;
+}
+
+__constant__ AesTables c_aes = make_aes_tables();
+
+__device__ __forceinline__ uint32_t ror8(uint32_t x) { return __byte_perm(x, x, 0x0321); }
+__device__ __forceinline__ uint32_t ror16(uint32_t x) { return __byte_perm(x, x, 0x1032); }
+__device__ __forceinline__ uint32_t ror24(uint32_t x) { return __byte_perm(x, x, 0x2103); }
+__device__ __forceinline__ uint32_t byte_of(uint32_t x, int b) { return __byte_perm(x, 0, 0x4440 | b); }
+
+// AES-128 key schedule (FIPS-197 5.2) from 16 key bytes at any address.
+__device__ inline void aes128_key_schedule(const uint8_t *key, uint32_t *rk) {
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+        rk[i] = ((uint32_t)key[4 * i] << 24) | ((uint32_t)key[4 * i + 1] << 16) | ((uint32_t)key[4 * i + 2] << 8) |
+                key[4 * i + 3];
+    uint32_t rcon = 1;
+#pragma unroll
+    for (int i = 4; i < 44; i++) {
+        uint32_t t = rk[i - 1];
+        if (i % 4 == 0) {
+            t = (t << 8) | (t >> 24);
+            t = ((uint32_t)c_aes.sbox[t >> 24] << 24) | ((uint32_t)c_aes.sbox[(t >> 16) & 0xFF] << 16) |
+                ((uint32_t)c_aes.sbox[(t >> 8) & 0xFF] << 8) | c_aes.sbox[t & 0xFF];
+            t ^= rcon << 24;
+            rcon = gf256_mulc((uint8_t)rcon, 2);
+        }
+        rk[i] = rk[i - 4] ^ t;
+    }
+}
+
+// Encrypt counter block `blk`; T points at the replicated table with this lane's column
+// already added (T + lane); rk in registers or shared.  Returns the 4 big-endian state words.
+struct AesOut {
+    uint32_t w0, w1, w2, w3;
+};
+template <class RK>
+__device__ __forceinline__ AesOut aes128_ctr_block(const uint32_t *T, const RK &rk, uint32_t blk) {
+#define TL(x) T[(x) << 5]
+    uint32_t s0 = rk[0], s1 = rk[1], s2 = rk[2], s3 = blk ^ rk[3];
+#pragma unroll
+    for (int r = 1; r < 10; r++) {
+        uint32_t t0 = TL(s0 >> 24) ^ ror8(TL(byte_of(s1, 2))) ^ ror16(TL(byte_of(s2, 1))) ^ ror24(TL(byte_of(s3, 0))) ^
+                      rk[4 * r];
+        uint32_t t1 = TL(s1 >> 24) ^ ror8(TL(byte_of(s2, 2))) ^ ror16(TL(byte_of(s3, 1))) ^ ror24(TL(byte_of(s0, 0))) ^
+                      rk[4 * r + 1];
+        uint32_t t2 = TL(s2 >> 24) ^ ror8(TL(byte_of(s3, 2))) ^ ror16(TL(byte_of(s0, 1))) ^ ror24(TL(byte_of(s1, 0))) ^
+                      rk[4 * r + 2];
+        uint32_t t3 = TL(s3 >> 24) ^ ror8(TL(byte_of(s0, 2))) ^ ror16(TL(byte_of(s1, 1))) ^ ror24(TL(byte_of(s2, 0))) ^
+                      rk[4 * r + 3];
+        s0 = t0;
+        s1 = t1;
+        s2 = t2;
+        s3 = t3;
+    }
+    // last round: S-box = byte 1 of T0[x]; gather four S-box bytes per output word with PRMT
+#define LASTW(a, b, c, d, k)                                                                   \
+    (__byte_perm(__byte_perm(TL((a) >> 24), TL(byte_of(b, 2)), 0x1500),                         \
+                 __byte_perm(TL(byte_of(c, 1)), TL(byte_of(d, 0)), 0x0015), 0x3254) ^            \
+     rk[k])
+    AesOut o;
+    o.w0 = LASTW(s0, s1, s2, s3, 40);
+    o.w1 = LASTW(s1, s2, s3, s0, 41);
+    o.w2 = LASTW(s2, s3, s0, s1, 42);
+    o.w3 = LASTW(s3, s0, s1, s2, 43);
+#undef LASTW
+#undef TL
+    return o;
+}
+
+// Big-endian words -> little-endian words of the byte stream.
+__device__ __forceinline__ uint32_t bswap32(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
+
+// Store 16 stream bytes (as 4 LE words) at any address, widest aligned stores possible.
+__device__ __forceinline__ void st16(uint8_t *p, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    uintptr_t ad = reinterpret_cast<uintptr_t>(p);
+    if ((ad & 15) == 0) {
+        *reinterpret_cast<uint4 *>(p) = make_uint4(a, b, c, d);
+    } else if ((ad & 7) == 0) {
+        reinterpret_cast<uint2 *>(p)[0] = make_uint2(a, b);
+        reinterpret_cast<uint2 *>(p)[1] = make_uint2(c, d);
+    } else if ((ad & 3) == 0) {
+        uint32_t *q = reinterpret_cast<uint32_t *>(p);
+        q[0] = a;
+        q[1] = b;
+        q[2] = c;
+        q[3] = d;
+    } else {
+        const uint32_t w[4] = {a, b, c, d};
+#pragma unroll
+        for (int i = 0; i < 16; i++) p[i] = (uint8_t)(w[i >> 2] >> (8 * (i & 3)));
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Kernel: AES-CTR keystream into a pitched pool.  grid = (chunks, batch); blocks
+// [0, nblk_main) of instance blockIdx.y go to row + out_off, keyed by 16 bytes at row + key_off.
+// When the key overlaps the output (expand-pk, expand-sk keep seed_pk in the last 16 output
+// bytes until expansion), nblk_main excludes the blocks that overlap the key and
+// aes_ctr_tail_kernel finishes them afterwards, one thread per instance.
+// ---------------------------------------------------------------------------------------------
+constexpr int AES_THREADS = 256;
+constexpr int AES_BLOCKS_PER_CTA = 2048;
+
+__global__ void __launch_bounds__(AES_THREADS) aes_ctr_kernel(uint8_t *pool, size_t pitch, size_t key_off,
+                                                               size_t out_off, uint32_t nblk_main) {
+    extern __shared__ uint32_t aes_smem[];  // 256 * 32 words
+    __shared__ uint32_t rk_s[44];
+    uint8_t *row = pool + (size_t)blockIdx.y * pitch;
+    for (int i = threadIdx.x; i < 256 * 32; i += AES_THREADS) aes_smem[i] = c_aes.te0[i >> 5];
+    if (threadIdx.x == 0) aes128_key_schedule(row + key_off, rk_s);
+    __syncthreads();
+    uint32_t rk[44];
+#pragma unroll
+    for (int i = 0; i < 44; i++) rk[i] = rk_s[i];
+    const uint32_t *T = aes_smem + (threadIdx.x & 31);
+    uint8_t *out = row + out_off;
+    const uint32_t b0 = blockIdx.x * AES_BLOCKS_PER_CTA;
+    const uint32_t b1 = min(b0 + AES_BLOCKS_PER_CTA, nblk_main);
+    for (uint32_t blk = b0 + threadIdx.x; blk < b1; blk += AES_THREADS) {
+        AesOut o = aes128_ctr_block(T, rk, blk);
+        st16(out + (size_t)blk * 16, bswap32(o.w0), bswap32(o.w1), bswap32(o.w2), bswap32(o.w3));
+    }
+}
+
+// Blocks [nblk_main, ceil(nbytes/16)) for each instance (key read before any byte is written).
+__global__ void aes_ctr_tail_kernel(uint8_t *pool, size_t pitch, size_t key_off, size_t out_off,
+                                    uint32_t nblk_main, uint32_t nbytes, uint32_t batch) {
+    uint32_t inst = blockIdx.x * blockDim.x + threadIdx.x;
+    if (inst >= batch) return;
+    uint8_t *row = pool + (size_t)inst * pitch;
+    uint32_t rk[44];
+    aes128_key_schedule(row + key_off, rk);
+    const uint32_t nblk = (nbytes + 15) / 16;
+    uint8_t buf[32];
+    for (uint32_t blk = nblk_main; blk < nblk; blk++) {
+        uint32_t s[4] = {0, 0, 0, blk};
+        // plain table walk through constant memory (at most two blocks per instance)
+        uint32_t s0 = s[0] ^ rk[0], s1 = s[1] ^ rk[1], s2 = s[2] ^ rk[2], s3 = s[3] ^ rk[3];
+        for (int r = 1; r < 10; r++) {
+            uint32_t t0 = c_aes.te0[s0 >> 24] ^ ror8(c_aes.te0[(s1 >> 16) & 255]) ^
+                          ror16(c_aes.te0[(s2 >> 8) & 255]) ^ ror24(c_aes.te0[s3 & 255]) ^ rk[4 * r];
+            uint32_t t1 = c_aes.te0[s1 >> 24] ^ ror8(c_aes.te0[(s2 >> 16) & 255]) ^
+                          ror16(c_aes.te0[(s3 >> 8) & 255]) ^ ror24(c_aes.te0[s0 & 255]) ^ rk[4 * r + 1];
+            uint32_t t2 = c_aes.te0[s2 >> 24] ^ ror8(c_aes.te0[(s3 >> 16) & 255]) ^
+                          ror16(c_aes.te0[(s0 >> 8) & 255]) ^ ror24(c_aes.te0[s1 & 255]) ^ rk[4 * r + 2];
+            uint32_t t3 = c_aes.te0[s3 >> 24] ^ ror8(c_aes.te0[(s0 >> 16) & 255]) ^
+                          ror16(c_aes.te0[(s1 >> 8) & 255]) ^ ror24(c_aes.te0[s2 & 255]) ^ rk[4 * r + 3];
+            s0 = t0;
+            s1 = t1;
+            s2 = t2;
+            s3 = t3;
+        }
+        const uint8_t *S = c_aes.sbox;
+        uint32_t o[4];
+        o[0] = ((uint32_t)S[s0 >> 24] << 24 | (uint32_t)S[(s1 >> 16) & 255] << 16 | (uint32_t)S[(s2 >> 8) & 255] << 8 |
+                S[s3 & 255]) ^ rk[40];
+        o[1] = ((uint32_t)S[s1 >> 24] << 24 | (uint32_t)S[(s2 >> 16) & 255] << 16 | (uint32_t)S[(s3 >> 8) & 255] << 8 |
+                S[s0 & 255]) ^ rk[41];
+        o[2] = ((uint32_t)S[s2 >> 24] << 24 | (uint32_t)S[(s3 >> 16) & 255] << 16 | (uint32_t)S[(s0 >> 8) & 255] << 8 |
+                S[s1 & 255]) ^ rk[42];
+        o[3] = ((uint32_t)S[s3 >> 24] << 24 | (uint32_t)S[(s0 >> 16) & 255] << 16 | (uint32_t)S[(s1 >> 8) & 255] << 8 |
+                S[s2 & 255]) ^ rk[43];
+        for (int i = 0; i < 16; i++) buf[(blk - nblk_main) * 16 + i] = (uint8_t)(o[i >> 2] >> (24 - 8 * (i & 3)));
+    }
+    // write only after every tail block is computed (the key may sit in these bytes)
+    uint8_t *out = row + out_off + (size_t)nblk_main * 16;
+    const uint32_t nb = nbytes - nblk_main * 16;
+    for (uint32_t i = 0; i < nb; i++) out[i] = buf[i];
+}
+
+}  // namespace mayo

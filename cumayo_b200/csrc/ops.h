@@ -1,0 +1,37 @@
+// ops.h -- internal launchers of the B200 MAYO engine (C++ linkage, not part of the C-ABI).
+// Every launcher takes the reference's pitched pool (row b = instance b) and byte offsets
+// inside a row; it launches asynchronously on `st` and returns a mayo_status code.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+namespace mayo {
+
+// Status codes shared with include/mayo_b200.h.
+enum : int {
+    ST_OK = 0,
+    ST_BAD_SET = 1,
+    ST_BAD_ARG = 2,
+    ST_CUDA = 3,
+};
+
+// Keypair of instances [0, batch): seed_sk = SHAKE128(LE64(rand_index + 2b + 1)).
+// Row layout (reference src/api.cu:17-26): sk @0, pk @A(SK), P1||P2 scratch @A(SK)+A(PK).
+int launch_keypair(int set, uint8_t *pool, size_t pitch, size_t batch, cudaStream_t st, uint64_t rand_index);
+// Keypair from caller seeds already stored at row offset 0 (sk_bytes each).
+int launch_keypair_seeded(int set, uint8_t *pool, size_t pitch, size_t batch, cudaStream_t st);
+// esk = sk || O || P1 || L in place over a row that holds sk at offset 0 (src/api.cu:47-54).
+int launch_expandsk(int set, uint8_t *pool, size_t pitch, size_t batch, cudaStream_t st);
+// epk = P1 || P2 || P3 in place over a row that holds cpk at offset P-16 (src/api.cu:64-77).
+int launch_expandpk(int set, uint8_t *pool, size_t pitch, size_t batch, cudaStream_t st);
+// Verify with epk at row offset 0; message, signature and result byte at the given offsets.
+int launch_verify(int set, uint8_t *pool, size_t pitch, size_t batch, cudaStream_t st, size_t mlen, size_t msg_off,
+                  size_t sig_off, size_t res_off);
+// Sign with esk at row offset 0; message and signature at the given offsets; `scratch_off`
+// points at the reference's per-row scratch (k*m*ceil(o/2) bytes) used as workspace.
+int launch_sign(int set, uint8_t *pool, size_t pitch, size_t batch, cudaStream_t st, size_t mlen, size_t msg_off,
+                size_t sig_off, size_t scratch_off);
+
+}  // namespace mayo

@@ -1,0 +1,134 @@
+/*
+ * mayo_b200.h -- C-ABI of the B200 batched MAYO engine (libmayo_b200.so).
+ *
+ * Drop-in boundary for SysuCrypto/cuMAYO's batched API.  Each mayo_b200_<name> below
+ * replaces the reference host function crypto_sign_<name> declared in include/api.cuh and
+ * implemented in src/api.cu of the reference project (line numbers cited per function),
+ * with the same pool layout, the same copies, the same argument order and asynchronous,
+ * stream-ordered semantics.  Differences, all additive:
+ *   - the MAYO parameter set (1, 2, 3 or 5) is the first argument instead of the
+ *     compile-time MAYO_VERSION, so all four sets live in one library;
+ *   - every function returns a mayo_b200_status instead of void;
+ *   - streams are passed as void* (a cudaStream_t; NULL = legacy default stream).
+ * include/api.cuh in this repository restores the reference's exact C++ signatures on top.
+ *
+ * Pools are caller-allocated, pitched device buffers: row b belongs to instance b.  Host
+ * buffers passed to the _HtD/_DtH helpers are tightly packed per instance, except where a
+ * function says otherwise (as in the reference).  The library never allocates memory.
+ */
+#ifndef MAYO_B200_H
+#define MAYO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MAYO_B200_API __attribute__((visibility("default")))
+#else
+#define MAYO_B200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MAYO_B200_ABI_VERSION 1
+
+typedef enum mayo_b200_status {
+    MAYO_B200_OK = 0,
+    MAYO_B200_ERR_SET = 1,  /* parameter set is not 1, 2, 3 or 5 */
+    MAYO_B200_ERR_ARG = 2,  /* null pointer, pitch too small, message too long, ... */
+    MAYO_B200_ERR_CUDA = 3, /* a CUDA call failed; see mayo_b200_last_cuda_error() */
+} mayo_b200_status;
+
+/* Byte sizes of one parameter set (reference include/params.h:10-92 and derived sizes). */
+typedef struct mayo_b200_sizes {
+    int32_t set, n, m, o, k, digest_bytes;
+    uint64_t sk_bytes;      /* compact secret key (seed_sk) */
+    uint64_t pk_bytes;      /* compact public key (seed_pk || P3) */
+    uint64_t sig_bytes;     /* k*n/2 + sk_bytes */
+    uint64_t esk_bytes;     /* seed_sk || O || P1 || L */
+    uint64_t epk_bytes;     /* P1 || P2 || P3 */
+    uint64_t p_bytes;       /* P1 || P2 */
+    uint64_t scratch_bytes; /* per-row sign scratch: k*m*ceil(o/2) */
+    /* minimum pool pitches for each reference entry point, for a message of mlen_hint */
+    uint64_t pitch_keypair, pitch_expandsk, pitch_expandpk;
+    uint64_t pitch_sign, pitch_sign_with_esk, pitch_verify;
+} mayo_b200_sizes;
+
+MAYO_B200_API int mayo_b200_abi_version(void);
+/* Sizes of `set`; pitches are computed for messages of `mlen_hint` bytes. */
+MAYO_B200_API int mayo_b200_get_sizes(int set, size_t mlen_hint, mayo_b200_sizes *out);
+/* Replaces aes128_tables_init() (reference include/aes128_ctr.cuh:16, src/aes128_ctr.cu:69-72).
+ * All tables are compile-time constants here; this only checks that the current device can
+ * run sm_100a code.  Calling it is optional. */
+MAYO_B200_API int mayo_b200_init(void);
+MAYO_B200_API const char *mayo_b200_status_string(int status);
+/* Last cudaError_t seen by this library on the calling thread (0 = none). */
+MAYO_B200_API int mayo_b200_last_cuda_error(void);
+
+/* ---- keypair: reference src/api.cu:17-38 ---- */
+/* Instance b uses seed_sk = SHAKE128(LE64(rand_index + 2b + 1)).  Row: sk @0, pk @A128(SK),
+ * P1||P2 scratch @A128(SK)+A128(PK). */
+MAYO_B200_API int mayo_b200_keypair(int set, uint8_t *pool, size_t pitch, size_t batch, void *stream,
+                                    size_t rand_index);
+MAYO_B200_API int mayo_b200_keypair_DtH(int set, uint8_t *pk, uint8_t *sk, const uint8_t *pool, size_t pitch,
+                                        size_t batch, void *stream);
+/* Extension: keypair from caller seeds already placed at row offset 0 (sk_bytes each),
+ * same row layout as mayo_b200_keypair. */
+MAYO_B200_API int mayo_b200_keypair_from_seed(int set, uint8_t *pool, size_t pitch, size_t batch, void *stream);
+
+/* ---- expand-sk: src/api.cu:40-62 (row: sk @0 -> esk in place) ---- */
+MAYO_B200_API int mayo_b200_expandsk_HtD(int set, const uint8_t *csk, uint8_t *pool, size_t pitch, size_t batch,
+                                         void *stream);
+MAYO_B200_API int mayo_b200_expandsk(int set, uint8_t *pool, size_t pitch, size_t batch, void *stream);
+MAYO_B200_API int mayo_b200_expandsk_DtH(int set, uint8_t *esk, const uint8_t *pool, size_t pitch, size_t batch,
+                                         void *stream);
+
+/* ---- expand-pk: src/api.cu:64-85 (row: cpk @P-16 -> epk = P1||P2||P3 @0) ---- */
+MAYO_B200_API int mayo_b200_expandpk_HtD(int set, const uint8_t *cpk, uint8_t *pool, size_t pitch, size_t batch,
+                                         void *stream);
+MAYO_B200_API int mayo_b200_expandpk(int set, uint8_t *pool, size_t pitch, size_t batch, void *stream);
+MAYO_B200_API int mayo_b200_expandpk_DtH(int set, uint8_t *epk, const uint8_t *pool, size_t pitch, size_t batch,
+                                         void *stream);
+
+/* ---- sign on an expanded key: src/api.cu:88-114 ----
+ * Row: esk @0, message @ESK, signature @ESK+mlen, scratch (k*m*ceil(o/2)) after it. */
+MAYO_B200_API int mayo_b200_sign_HtD(int set, const uint8_t *esk, const uint8_t *msg, size_t mlen, uint8_t *pool,
+                                     size_t pitch, size_t batch, void *stream);
+MAYO_B200_API int mayo_b200_sign(int set, uint8_t *pool, size_t mlen, size_t pitch, size_t batch, void *stream);
+MAYO_B200_API int mayo_b200_sign_DtH(int set, uint8_t *sig, const uint8_t *pool, size_t mlen, size_t pitch,
+                                     size_t batch, void *stream);
+
+/* ---- sign from a compact key: src/api.cu:116-144 ----
+ * Row: sk @0 (expanded in place), message @A(ESK), signature @A(ESK)+A(mlen), scratch after
+ * A(SIG).  A(x) = x rounded up to 128. */
+MAYO_B200_API int mayo_b200_signWithesk_HtD(int set, const uint8_t *csk, const uint8_t *msg, size_t mlen,
+                                            uint8_t *pool, size_t pitch, size_t batch, void *stream);
+MAYO_B200_API int mayo_b200_signWithesk(int set, uint8_t *pool, size_t mlen, size_t pitch, size_t batch,
+                                        void *stream);
+MAYO_B200_API int mayo_b200_signWithesk_DtH(int set, uint8_t *sig, const uint8_t *pool, size_t mlen, size_t pitch,
+                                            size_t batch, void *stream);
+
+/* ---- verify on an expanded key: src/api.cu:146-178 ----
+ * Row: epk @0, message @A(EPK), signature @A(EPK)+A(mlen), result byte @+A(SIG)
+ * (0 = accept, 1 = reject).  _HtD reads epk and sig with 128-byte-aligned host strides. */
+MAYO_B200_API int mayo_b200_verify_HtD(int set, const uint8_t *epk, const uint8_t *msg, const uint8_t *sig,
+                                       size_t mlen, uint8_t *pool, size_t pitch, size_t batch, void *stream);
+MAYO_B200_API int mayo_b200_verify(int set, uint8_t *pool, size_t mlen, size_t pitch, size_t batch, void *stream);
+MAYO_B200_API int mayo_b200_verify_DtH(int set, uint8_t *result, size_t mlen, const uint8_t *pool, size_t pitch,
+                                       size_t batch, void *stream);
+
+/* ---- verify from a compact key: src/api.cu:180-218 (cpk lands @P-16, then expanded) ---- */
+MAYO_B200_API int mayo_b200_verifyWithepk_HtD(int set, const uint8_t *cpk, const uint8_t *msg, const uint8_t *sig,
+                                              size_t mlen, uint8_t *pool, size_t pitch, size_t batch,
+                                              void *stream);
+MAYO_B200_API int mayo_b200_verifyWithepk(int set, uint8_t *pool, size_t mlen, size_t pitch, size_t batch,
+                                          void *stream);
+MAYO_B200_API int mayo_b200_verifyWithepk_DtH(int set, uint8_t *result, size_t mlen, const uint8_t *pool,
+                                              size_t pitch, size_t batch, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MAYO_B200_H */
