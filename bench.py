@@ -1,0 +1,504 @@
+#!/usr/bin/env python3
+"""Throughput benchmark of the B200 MAYO engine (and of the reference, --impl reference).
+
+Default workload (one GPU): MAYO_2 shared-key sign and verify, batch 65,536.  One seeded
+keypair is expanded once and stays resident in HBM; every instance signs its own message
+(length uniform in [32, 1024] bytes, bytes from a seeded ChaCha20 stream) and the batch of
+signatures is then verified.  A step = sign the batch + verify the batch; `value` counts
+both operations.  Other workloads (--workload): c1 = MAYO_1 keypair -> sign -> verify, batch
+1,024, distinct keys; c3-3 / c3-5 = MAYO_3 / MAYO_5 distinct-key verify, batch 16,384, 10%
+corrupted signatures.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2]
+
+Prints one JSON line (rank 0).  Under torchrun each rank runs the same per-GPU workload on
+its own GPU (weak scaling, no collective on the data path); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "sign/s and verify/s per B200 (MAYO_1/2/3/5), byte-exact; serving p50/p99 vs plain"
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+LOP3_LANE_OPS_PER_CLK_SM = 64  # measured on this pool's B200 (profiles/int_pipes_b200.md)
+A128 = lambda x: (x + 127) // 128 * 128  # noqa: E731
+
+# ---------------------------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------------------------
+WORKLOADS = {
+    "c2": dict(set=2, batch=65536, kind="shared_sign_verify", mlen=(32, 1024)),
+    "c1": dict(set=1, batch=1024, kind="keypair_sign_verify", mlen=(32, 32)),
+    "c3-3": dict(set=3, batch=16384, kind="distinct_verify", mlen=(32, 32)),
+    "c3-5": dict(set=5, batch=16384, kind="distinct_verify", mlen=(32, 32)),
+}
+
+PARAMS = {1: (86, 78, 8, 10), 2: (81, 64, 17, 4), 3: (118, 108, 10, 11), 5: (154, 142, 12, 12)}
+
+
+def mac_counts(s: int) -> dict:
+    """Algorithmic GF(16) multiply-accumulates per operation (coordinate x scalar)."""
+    n, m, o, k = PARAMS[s]
+    v = n - o
+    e1, e2, e3 = v * (v + 1) // 2, v * o, o * (o + 1) // 2
+    sign = k * m * e1 + m * k * k * v + k * m * v * o + m * m * (k * o + 1)
+    verify = k * m * (e1 + e2 + e3) + m * k * k * n
+    keypair = o * m * (e1 + e2) + m * o * o * v
+    return dict(sign=sign, verify=verify, keypair=keypair)
+
+
+def chacha(key: bytes, n: int) -> np.ndarray:
+    from cryptography.hazmat.primitives.ciphers import Cipher, algorithms
+    enc = Cipher(algorithms.ChaCha20(key, b"\0" * 16), mode=None).encryptor()
+    return np.frombuffer(enc.update(b"\0" * n), dtype=np.uint8)
+
+
+def make_messages(seed: int, batch: int, lo: int, hi: int):
+    """Seeded ChaCha20 stream: lengths uniform in [lo, hi], then message bytes."""
+    key = (b"mayo-b200-bench-%d" % seed).ljust(32, b"\0")[:32]
+    raw = chacha(key, 4 * batch)
+    lens = (lo + (raw.view(np.uint32) % np.uint32(hi - lo + 1))).astype(np.uint32)
+    offs = np.zeros(batch, np.uint64)
+    offs[1:] = np.cumsum(lens[:-1], dtype=np.uint64)
+    total = int(lens.sum())
+    body = chacha(key[::-1], total + 16)[16:16 + total].copy()
+    return body, offs, lens
+
+
+def seeds_for(seed: int, batch: int, skb: int) -> np.ndarray:
+    key = (b"mayo-b200-keys-%d" % seed).ljust(32, b"\0")[:32]
+    return chacha(key, batch * skb).reshape(batch, skb).copy()
+
+
+# ---------------------------------------------------------------------------------------------
+# distributed plumbing (one process per GPU)
+# ---------------------------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            import torch
+            self.pg.barrier(device_ids=[self.local])
+            torch.cuda.synchronize()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = os.path.join("/tmp", f"mayo_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------
+# our engine
+# ---------------------------------------------------------------------------------------------
+def run_ours(args, dist: Dist):
+    import torch
+
+    import cumayo_b200 as M
+
+    wl = WORKLOADS[args.workload]
+    s, batch = wl["set"], args.batch or wl["batch"]
+    m = M.Mayo(s)
+    z = m.sizes
+    dev = torch.device("cuda", dist.local)
+    torch.cuda.set_device(dev)
+    st = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    launches_per_step = 0
+    seed = 1 + dist.rank
+
+    if wl["kind"] == "shared_sign_verify":
+        # one resident expanded key (esk, epk), messages of per-instance length
+        sk_seed = seeds_for(seed, 1, z.sk_bytes)
+        kp, kpitch = m.alloc_pool("keypair", 1)
+        kp[: z.sk_bytes].copy_(torch.from_numpy(sk_seed[0]))
+        m.crypto_sign_keypair_from_seed(kp, kpitch, 1, st)
+        esk = torch.zeros(z.esk_bytes, dtype=torch.uint8, device=dev)
+        esk[: z.sk_bytes].copy_(kp[: z.sk_bytes])
+        m.crypto_sign_expandsk(esk, z.esk_bytes, 1, st)
+        epk = torch.zeros(z.epk_bytes, dtype=torch.uint8, device=dev)
+        pk_off = A128(z.sk_bytes)
+        epk[z.p_bytes - 16: z.p_bytes - 16 + z.pk_bytes].copy_(kp[pk_off: pk_off + z.pk_bytes])
+        m.crypto_sign_expandpk(epk, z.epk_bytes, 1, st)
+        body, offs, lens = make_messages(seed, batch, *wl["mlen"])
+        h_msgs = torch.from_numpy(body).pin_memory()
+        h_offs = torch.from_numpy(offs.view(np.int64)).pin_memory()
+        h_lens = torch.from_numpy(lens.view(np.int32)).pin_memory()
+        d_msgs = h_msgs.to(dev)
+        d_offs = h_offs.to(dev)
+        d_lens = h_lens.to(dev)
+        sig = torch.zeros(batch * z.sig_bytes, dtype=torch.uint8, device=dev)
+        ws = torch.zeros(batch * m.sign_ws_bytes(), dtype=torch.uint8, device=dev)
+        res = torch.zeros(batch, dtype=torch.uint8, device=dev)
+        h_sig = torch.zeros(batch * z.sig_bytes, dtype=torch.uint8).pin_memory()
+        h_res = torch.zeros(batch, dtype=torch.uint8).pin_memory()
+        launches_per_step = 3  # sign: hash + core; verify: one
+
+        def sign_op():
+            m.sign_many(esk, d_msgs, sig, ws, batch, msg_off=d_offs, msg_len=d_lens, stream=st)
+
+        def verify_op():
+            m.verify_many(epk, d_msgs, sig, res, batch, msg_off=d_offs, msg_len=d_lens, stream=st)
+
+        def h2d():
+            d_msgs.copy_(h_msgs, non_blocking=True)
+            d_offs.copy_(h_offs, non_blocking=True)
+            d_lens.copy_(h_lens, non_blocking=True)
+
+        def d2h():
+            h_sig.copy_(sig, non_blocking=True)
+            h_res.copy_(res, non_blocking=True)
+
+        h2d_bytes = body.nbytes + offs.nbytes + lens.nbytes
+        d2h_bytes = batch * z.sig_bytes + batch
+        phases = [("sign", sign_op), ("verify", verify_op)]
+        ops_per_step = 2 * batch
+        macs = mac_counts(s)
+        work = {"sign": macs["sign"] * batch, "verify": macs["verify"] * batch}
+        hbm_bytes = {"sign": z.esk_bytes + body.nbytes + batch * (z.sig_bytes + 2 * m.sign_ws_bytes()),
+                     "verify": z.epk_bytes + body.nbytes + batch * (z.sig_bytes + 1)}
+        cfg = {"workload": "MAYO_2 shared-key sign+verify", "set": "MAYO_2", "batch": batch,
+               "msg_len": "uniform 32..1024 B", "key": "one expanded key resident in HBM",
+               "l2": "flushed between steps (256 MiB write)", "api": "mayo_b200_sign_many / verify_many"}
+        check = lambda: int(res.sum().item())  # noqa: E731  (must be 0: every signature accepted)
+    else:
+        raise SystemExit(f"workload {args.workload} not implemented in this arm yet")
+
+    def step():
+        flush.fill_(1)
+        for _, fn in phases:
+            fn()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    bad = check()
+
+    # ---- device-resident timing ----
+    ev = {name: [] for name, _ in phases}
+    clocks = Clocks(dist.local)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(st)
+    for _ in range(args.steps):
+        flush.fill_(1)
+        for name, fn in phases:
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            fn()
+            b.record(st)
+            ev[name].append((a, b))
+    t1.record(st)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    total_ms = dist.max(t0.elapsed_time(t1))
+    phase_ms = {name: sum(a.elapsed_time(b) for a, b in lst) / len(lst) for name, lst in ev.items()}
+
+    # ---- end to end through the public API with host buffers ----
+    dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(args.steps):
+        flush.fill_(1)
+        h2d()
+        for _, fn in phases:
+            fn()
+        d2h()
+    e1.record(st)
+    torch.cuda.synchronize()
+    e2e_ms = dist.max(e0.elapsed_time(e1))
+    bad_e2e = int(h_res.sum().item())
+
+    ms_per_step = total_ms / args.steps
+    value = ops_per_step * dist.world / (ms_per_step / 1e3)
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    peak_ops = LOP3_LANE_OPS_PER_CLK_SM * 148 * sm_mhz * 1e6 / 1e9  # G lane-ops/s
+    dom = max(phase_ms, key=phase_ms.get)
+    ach_ops = 0.5 * work[dom] / (phase_ms[dom] / 1e3) / 1e9  # 16 LOP3 per 32 GF(16) MACs
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": "ops/s", "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 (GF(16) bit-planes)", "data": "synthetic (seeded ChaCha20)",
+        "config": cfg,
+        "sign_per_s": round(batch * dist.world / (phase_ms["sign"] / 1e3), 1) if "sign" in phase_ms else None,
+        "verify_per_s": round(batch * dist.world / (phase_ms["verify"] / 1e3), 1) if "verify" in phase_ms else None,
+        "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
+        "roofline": {"bound": "alu", "kernel": f"{dom} ({args.workload})", "achieved": round(ach_ops, 1),
+                     "peak": round(peak_ops, 1), "unit": "G int-ops/s", "frac": round(ach_ops / peak_ops, 4),
+                     "traffic": None,
+                     "definition": "algorithmic ops = 0.5 x GF(16) MACs (16 LOP3 per 32 MACs); peak = measured "
+                                   "LOP3 issue rate 64 lane-ops/clk/SM x 148 SMs x median SM clock"},
+        "roofline_hbm": {"bound": "hbm", "achieved": round(hbm_bytes[dom] / (phase_ms[dom] / 1e3) / 1e9, 2),
+                         "peak": 6550.1, "unit": "GB/s",
+                         "frac": round(hbm_bytes[dom] / (phase_ms[dom] / 1e3) / 1e9 / 6550.1, 5)},
+        "e2e": {"value": round(ops_per_step * dist.world / (e2e_ms / args.steps / 1e3), 1), "unit": "ops/s",
+                "h2d_bytes_per_step": int(h2d_bytes), "d2h_bytes_per_step": int(d2h_bytes)},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk,
+        "rejected_valid_signatures": bad + bad_e2e,
+    }
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args)
+    return out
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU baseline: the oracle (a restatement of the reference's algorithm) on the host cores
+# ---------------------------------------------------------------------------------------------
+def cpu_baseline(args, sample: int | None = None):
+    from oracle import oracle as O
+    wl = WORKLOADS[args.workload]
+    s = wl["set"]
+    P = O.params(s)
+    threads = O.max_threads()
+    if wl["kind"] == "shared_sign_verify":
+        sample = sample or 4096
+        seed = seeds_for(1, 1, P.sk_bytes)[0].tobytes()
+        pk = O.keypair_from_seed(s, seed)
+        esk = np.frombuffer(O.expandsk(s, seed), np.uint8)[None, :]
+        epk = np.frombuffer(O.expandpk(s, pk), np.uint8)[None, :]
+        body, offs, lens = make_messages(1, sample, *wl["mlen"])
+        msgs = [body[int(o):int(o) + int(n)].tobytes() for o, n in zip(offs, lens)]
+        t = time.perf_counter()
+        sig, _ = O.sign_batch(s, esk, msgs, shared_key=True)
+        t_sign = time.perf_counter() - t
+        t = time.perf_counter()
+        res = O.verify_batch(s, epk, msgs, sig, shared_key=True)
+        t_ver = time.perf_counter() - t
+        assert int(res.sum()) == 0
+        return {"value": round(2 * sample / (t_sign + t_ver), 1), "unit": "ops/s", "cores": threads, "kind": "port",
+                "sample": f"{sample} signs + {sample} verifies of the same workload (shared MAYO_2 key, "
+                          f"32..1024 B messages), OpenMP one instance per thread",
+                "sign_per_s": round(sample / t_sign, 1), "verify_per_s": round(sample / t_ver, 1)}
+    return None
+
+
+# ---------------------------------------------------------------------------------------------
+# reference arm: the reference's own CUDA build (oracle/_ref) through its own API
+# ---------------------------------------------------------------------------------------------
+def run_reference(args, dist: Dist):
+    import ctypes
+
+    import torch
+    wl = WORKLOADS[args.workload]
+    s, batch = wl["set"], args.batch or wl["batch"]
+    path = os.path.join(ROOT, "oracle", "_ref", f"libref_mayo{s}.so")
+    if not os.path.exists(path):
+        return {"impl": "reference", "unavailable": f"{path} not built (make -C oracle ref needs the reference sources)"}
+    if wl["kind"] != "shared_sign_verify":
+        return {"impl": "reference", "unavailable": f"reference arm for {args.workload} not implemented"}
+    L = ctypes.CDLL(path)
+    vp, sz = ctypes.c_void_p, ctypes.c_size_t
+    for f in ("ref_sign", "ref_verify"):
+        getattr(L, f).argtypes = [vp, sz, sz, sz, vp]
+    L.ref_keypair.argtypes = [vp, sz, sz, vp, sz]
+    L.ref_expandsk.argtypes = [vp, sz, sz, vp]
+    L.ref_expandpk.argtypes = [vp, sz, sz, vp]
+    L.ref_init()
+    torch.cuda.set_device(dist.local)
+    dev = torch.device("cuda", dist.local)
+    from oracle import oracle as O
+    P = O.params(s)
+    # the shared key, expanded by the reference itself, then replicated into every pool row
+    seed = seeds_for(1 + dist.rank, 1, P.sk_bytes)[0]
+    pk = np.frombuffer(O.keypair_from_seed(s, seed.tobytes()), np.uint8)
+    kp = torch.zeros(P.esk_bytes + 64, dtype=torch.uint8, device=dev)
+    kp[: P.sk_bytes].copy_(torch.from_numpy(seed))
+    L.ref_expandsk(kp.data_ptr(), P.esk_bytes, 1, None)
+    esk = kp[: P.esk_bytes].clone()
+    kq = torch.zeros(P.epk_bytes + 64, dtype=torch.uint8, device=dev)
+    kq[P.p_bytes - 16: P.p_bytes - 16 + P.pk_bytes].copy_(torch.from_numpy(pk))
+    L.ref_expandpk(kq.data_ptr(), P.epk_bytes, 1, None)
+    epk = kq[: P.epk_bytes].clone()
+    body, offs, lens = make_messages(1 + dist.rank, batch, *wl["mlen"])
+    order = np.argsort(lens, kind="stable")
+    maxlen = int(lens.max())
+    sp = (P.esk_bytes + maxlen + P.sig_bytes + P.k * P.m * ((P.o + 1) // 2) + 511) // 512 * 512
+    vpch = (A128(P.epk_bytes) + A128(maxlen) + A128(P.sig_bytes) + 1 + 511) // 512 * 512
+    spool = torch.zeros((batch, sp), dtype=torch.uint8, device=dev)
+    vpool = torch.zeros((batch, vpch), dtype=torch.uint8, device=dev)
+    spool[:, : P.esk_bytes].copy_(esk.expand(batch, -1))
+    vpool[:, : P.epk_bytes].copy_(epk.expand(batch, -1))
+    groups = []
+    i = 0
+    slens = lens[order]
+    while i < batch:
+        j = i
+        while j < batch and slens[j] == slens[i]:
+            j += 1
+        groups.append((i, j - i, int(slens[i])))
+        i = j
+    # messages into the rows (sorted by length), the reference's sign layout: msg @ESK
+    for r, src in enumerate(order):
+        o, n = int(offs[src]), int(lens[src])
+        spool[r, P.esk_bytes: P.esk_bytes + n] = torch.from_numpy(body[o:o + n])
+        vpool[r, A128(P.epk_bytes): A128(P.epk_bytes) + n] = torch.from_numpy(body[o:o + n])
+    streams = [torch.cuda.Stream(device=dev) for _ in range(10)]
+
+    def sign_all():
+        for g, (r0, cnt, L_) in enumerate(groups):
+            L.ref_sign(spool[r0].data_ptr(), L_, sp, cnt, streams[g % 10].cuda_stream)
+
+    def copy_sigs():
+        # reference verify layout: sig @A(EPK) + A(Mlen) (per-group offset)
+        for r0, cnt, L_ in groups:
+            so = P.esk_bytes + L_
+            vo = A128(P.epk_bytes) + A128(L_)
+            vpool[r0:r0 + cnt, vo: vo + P.sig_bytes].copy_(spool[r0:r0 + cnt, so: so + P.sig_bytes])
+
+    def verify_all():
+        for g, (r0, cnt, L_) in enumerate(groups):
+            L.ref_verify(vpool[r0].data_ptr(), L_, vpch, cnt, streams[g % 10].cuda_stream)
+
+    def timed(fn) -> float:
+        cur = torch.cuda.current_stream()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(cur)
+        for sx in streams:
+            sx.wait_event(a)
+        fn()
+        for sx in streams:
+            e = torch.cuda.Event()
+            e.record(sx)
+            cur.wait_event(e)
+        b.record(cur)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    for _ in range(args.warmup):
+        timed(sign_all)
+        copy_sigs()
+        torch.cuda.synchronize()
+        timed(verify_all)
+    dist.barrier()
+    ts, tv = [], []
+    for _ in range(args.steps):
+        ts.append(timed(sign_all))
+        copy_sigs()
+        torch.cuda.synchronize()
+        tv.append(timed(verify_all))
+    dist.barrier()
+    res_off = [A128(P.epk_bytes) + A128(L_) + A128(P.sig_bytes) for _, _, L_ in groups]
+    bad = 0
+    for (r0, cnt, _), ro in zip(groups, res_off):
+        bad += int(vpool[r0:r0 + cnt, ro].sum().item())
+    ms = dist.max((sum(ts) + sum(tv)) / args.steps)
+    value = 2 * batch * dist.world / (ms / 1e3)
+    return {"metric": METRIC, "value": round(value, 1), "unit": "ops/s", "impl": "reference", "n_gpus": dist.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded ChaCha20)",
+            "config": {"workload": "MAYO_2 shared-key sign+verify", "set": "MAYO_2", "batch": batch,
+                       "msg_len": "uniform 32..1024 B",
+                       "key": "expanded key replicated in every pool row (the reference API has no shared key)",
+                       "api": "crypto_sign_sign / crypto_sign_verify, one launch per message length, "
+                              "round-robin over 10 streams (the reference benchmark's stream pattern)"},
+            "sign_per_s": round(batch * dist.world / (sum(ts) / len(ts) / 1e3), 1),
+            "verify_per_s": round(batch * dist.world / (sum(tv) / len(tv) / 1e3), 1),
+            "launches_per_step": 2 * len(groups), "rejected_valid_signatures": bad,
+            "cpu_baseline": {"value": round(value, 1), "unit": "ops/s", "cores": 0, "kind": "reference",
+                             "sample": "not a CPU run: the reference has no CPU implementation; this arm times "
+                                       "its own CUDA build on the same B200"},
+            "e2e": {"value": round(value, 1), "unit": "ops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    dist = Dist()
+    try:
+        out = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
+    finally:
+        dist.close()
+    if dist.rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

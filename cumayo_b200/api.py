@@ -83,6 +83,13 @@ def lib() -> ctypes.CDLL:
         L.mayo_b200_abi_version.restype = ctypes.c_int
         L.mayo_b200_init.restype = ctypes.c_int
         L.mayo_b200_last_cuda_error.restype = ctypes.c_int
+        L.mayo_b200_sign_ws_bytes.restype = ctypes.c_size_t
+        L.mayo_b200_sign_ws_bytes.argtypes = [ctypes.c_int]
+        vp, sz = ctypes.c_void_p, ctypes.c_size_t
+        L.mayo_b200_sign_many.restype = ctypes.c_int
+        L.mayo_b200_sign_many.argtypes = [ctypes.c_int, vp, sz, vp, vp, vp, sz, sz, vp, sz, vp, sz, vp]
+        L.mayo_b200_verify_many.restype = ctypes.c_int
+        L.mayo_b200_verify_many.argtypes = [ctypes.c_int, vp, sz, vp, vp, vp, sz, sz, vp, sz, vp, sz, vp]
         _lib = L
     return _lib
 
@@ -259,6 +266,27 @@ class Mayo:
     def crypto_sign_verifyWithepk_DtH(self, verify, Mlen, pool, pitch, batch_size, stream=None):
         _check(lib().mayo_b200_verifyWithepk_DtH(self.set, _ptr(verify), Mlen, _ptr(pool), pitch, batch_size,
                                                  _stream(stream)), "crypto_sign_verifyWithepk_DtH")
+
+    # extension: explicit operand arrays (shared keys, per-instance message lengths) --------
+    def sign_ws_bytes(self) -> int:
+        return int(lib().mayo_b200_sign_ws_bytes(self.set))
+
+    def sign_many(self, esk, msgs, sig, ws, batch, *, msg_off=None, msg_len=None, msg_stride=0, mlen=0,
+                  esk_stride=0, sig_stride=None, stream=None):
+        """Sign `batch` messages (device operands).  esk_stride=0 shares one expanded key."""
+        z = self.sizes
+        _check(lib().mayo_b200_sign_many(self.set, _ptr(esk), esk_stride, _ptr(msgs), _ptr(msg_off), _ptr(msg_len),
+                                         msg_stride, mlen, _ptr(sig), z.sig_bytes if sig_stride is None else sig_stride,
+                                         _ptr(ws), batch, _stream(stream)), "sign_many")
+
+    def verify_many(self, epk, msgs, sig, result, batch, *, msg_off=None, msg_len=None, msg_stride=0, mlen=0,
+                    epk_stride=0, sig_stride=None, stream=None):
+        """Verify `batch` signatures (device operands); result[i] = 0 accept, 1 reject."""
+        z = self.sizes
+        _check(lib().mayo_b200_verify_many(self.set, _ptr(epk), epk_stride, _ptr(msgs), _ptr(msg_off),
+                                           _ptr(msg_len), msg_stride, mlen, _ptr(sig),
+                                           z.sig_bytes if sig_stride is None else sig_stride, _ptr(result), batch,
+                                           _stream(stream)), "verify_many")
 
     # pools (the reference benchmark's sizes, tests/bench_stream.cu:25-31, 82, 133) ----------
     def pool_bytes(self, kind: str, mlen: int = 0) -> int:

@@ -323,4 +323,39 @@ MAYO_B200_API int mayo_b200_verifyWithepk_DtH(int set, uint8_t *result, size_t m
     return mayo_b200_verify_DtH(set, result, mlen, pool, pitch, batch, stream);
 }
 
+// ---- extension: explicit operand arrays ----
+MAYO_B200_API size_t mayo_b200_sign_ws_bytes(int set) { return sign_ws_bytes(set); }
+
+MAYO_B200_API int mayo_b200_sign_many(int set, const uint8_t *esk, size_t esk_stride, const uint8_t *msgs,
+                                      const uint64_t *msg_off, const uint32_t *msg_len, size_t msg_stride,
+                                      size_t mlen, uint8_t *sig, size_t sig_stride, uint8_t *ws, size_t batch,
+                                      void *stream) {
+    Sz z;
+    if (!sizes_of(set, z)) return MAYO_B200_ERR_SET;
+    if (batch == 0) return MAYO_B200_OK;
+    if (!esk || !sig || !ws || batch > 0x7fffffffu || mlen > 0x7fffffffu) return MAYO_B200_ERR_ARG;
+    if ((msg_off == nullptr) != (msg_len == nullptr)) return MAYO_B200_ERR_ARG;
+    if (!msgs && (msg_off || mlen)) return MAYO_B200_ERR_ARG;
+    if (batch > 1 && sig_stride < z.sig) return MAYO_B200_ERR_ARG;
+    SignIO io{esk, esk_stride, MsgIO{msgs, msg_stride, msg_off, msg_len, (uint32_t)mlen}, sig, sig_stride, ws,
+              sign_ws_bytes(set)};
+    return kernel_rc(launch_sign_io(set, io, batch, S_(stream)));
+}
+
+MAYO_B200_API int mayo_b200_verify_many(int set, const uint8_t *epk, size_t epk_stride, const uint8_t *msgs,
+                                        const uint64_t *msg_off, const uint32_t *msg_len, size_t msg_stride,
+                                        size_t mlen, const uint8_t *sig, size_t sig_stride, uint8_t *result,
+                                        size_t batch, void *stream) {
+    Sz z;
+    if (!sizes_of(set, z)) return MAYO_B200_ERR_SET;
+    if (batch == 0) return MAYO_B200_OK;
+    if (!epk || !sig || !result || batch > 0x7fffffffu || mlen > 0x7fffffffu) return MAYO_B200_ERR_ARG;
+    if ((msg_off == nullptr) != (msg_len == nullptr)) return MAYO_B200_ERR_ARG;
+    if (!msgs && (msg_off || mlen)) return MAYO_B200_ERR_ARG;
+    if (batch > 1 && sig_stride < z.sig) return MAYO_B200_ERR_ARG;
+    VerifyIO io{epk, epk_stride, MsgIO{msgs, msg_stride, msg_off, msg_len, (uint32_t)mlen}, sig, sig_stride, result,
+                1};
+    return kernel_rc(launch_verify_io(set, io, batch, S_(stream)));
+}
+
 }  // extern "C"

@@ -31,20 +31,18 @@ struct SignWs {
 };
 
 template <int SET>
-__global__ void sign_hash_kernel(uint8_t *pool, size_t pitch, uint32_t batch, uint32_t mlen, size_t msg_off,
-                                 size_t ws_off) {
+__global__ void sign_hash_kernel(const SignIO io, uint32_t batch) {
     using S = Set<SET>;
     using WS = SignWs<SET>;
     const uint32_t inst = blockIdx.x * blockDim.x + threadIdx.x;
     if (inst >= batch) return;
-    uint8_t *row = pool + (size_t)inst * pitch;
-    const uint8_t *seed_sk = row;
-    uint8_t *ws = row + ws_off;
+    const uint8_t *seed_sk = io.esk + (size_t)inst * io.esk_stride;
+    uint8_t *ws = io.ws + (size_t)inst * io.ws_stride;
     uint8_t digest[S::digest], salt[S::sk];
     {
         Sponge<136> sp;  // digest = SHAKE256(M) (sign.cu:225)
         sp.init();
-        sp.absorb(row + msg_off, mlen);
+        sp.absorb(io.m.ptr(inst), io.m.len(inst));
         sp.finalize();
         sp.squeeze(digest, S::digest);
     }
@@ -162,8 +160,7 @@ __device__ __forceinline__ uint32_t zdown_word(const uint32_t *u, int q, int shi
 }
 
 template <int SET>
-__global__ void __launch_bounds__(SignCfg<SET>::NT) sign_kernel(uint8_t *pool, size_t pitch, size_t sig_off,
-                                                                 size_t ws_off) {
+__global__ void __launch_bounds__(SignCfg<SET>::NT) sign_kernel(const SignIO io) {
     using S = Set<SET>;
     using C = SignCfg<SET>;
     using WS = SignWs<SET>;
@@ -186,14 +183,15 @@ __global__ void __launch_bounds__(SignCfg<SET>::NT) sign_kernel(uint8_t *pool, s
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
-    uint8_t *row = pool + (size_t)blockIdx.x * pitch;
-    const uint8_t *O_g = row + S::sk;
-    const uint8_t *P1 = row + S::sk + S::o_bytes;
+    const size_t inst = blockIdx.x;
+    const uint8_t *esk = io.esk + inst * io.esk_stride;
+    const uint8_t *O_g = esk + S::sk;
+    const uint8_t *P1 = esk + S::sk + S::o_bytes;
     const uint8_t *L = P1 + S::p1;
-    const uint8_t *ws = row + ws_off;
+    const uint8_t *ws = io.ws + inst * io.ws_stride;
 
     for (int i = tid; i < S::digest + S::sk; i += NT) s_key[i] = ws[WS::dig + i];
-    for (int i = tid; i < S::sk; i += NT) s_key[S::digest + S::sk + i] = row[i];
+    for (int i = tid; i < S::sk; i += NT) s_key[S::digest + S::sk + i] = esk[i];
     for (int i = tid; i < NW * 4; i += NT) s_t[i] = i < S::menc ? ws[WS::t + i] : 0;
     for (int i = tid; i < S::vr; i += NT) s_vr[i] = ws[WS::vr + i];
     __syncthreads();
@@ -496,7 +494,7 @@ __global__ void __launch_bounds__(SignCfg<SET>::NT) sign_kernel(uint8_t *pool, s
     }
 
     // ---- s = V + O x, then salt (sign.cu:147-191, 474-477) ----
-    uint8_t *sigp = row + sig_off;
+    uint8_t *sigp = io.sig + inst * io.sig_stride;
     for (int bidx = tid; bidx < S::k * S::n / 2; bidx += NT) {
         uint32_t nb[2];
 #pragma unroll
@@ -524,26 +522,40 @@ __global__ void __launch_bounds__(SignCfg<SET>::NT) sign_kernel(uint8_t *pool, s
 }
 
 template <int SET>
-static int sign_t(uint8_t *pool, size_t pitch, size_t batch, cudaStream_t st, size_t mlen, size_t msg_off,
-                  size_t sig_off, size_t scratch_off) {
+static int sign_t(const SignIO &io, size_t batch, cudaStream_t st) {
     using C = SignCfg<SET>;
-    sign_hash_kernel<SET><<<(unsigned)((batch + 127) / 128), 128, 0, st>>>(pool, pitch, (uint32_t)batch,
-                                                                             (uint32_t)mlen, msg_off, scratch_off);
+    sign_hash_kernel<SET><<<(unsigned)((batch + 127) / 128), 128, 0, st>>>(io, (uint32_t)batch);
     if (!set_smem_attr(sign_kernel<SET>, C::total)) return ST_CUDA;
-    sign_kernel<SET><<<(unsigned)batch, C::NT, C::total, st>>>(pool, pitch, sig_off, scratch_off);
+    sign_kernel<SET><<<(unsigned)batch, C::NT, C::total, st>>>(io);
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+int launch_sign_io(int set, const SignIO &io, size_t batch, cudaStream_t st) {
+    if (batch == 0) return ST_OK;
+    switch (set) {
+        case 1: return sign_t<1>(io, batch, st);
+        case 2: return sign_t<2>(io, batch, st);
+        case 3: return sign_t<3>(io, batch, st);
+        case 5: return sign_t<5>(io, batch, st);
+        default: return ST_BAD_SET;
+    }
+}
+
+size_t sign_ws_bytes(int set) {
+    switch (set) {
+        case 1: return SignWs<1>::total;
+        case 2: return SignWs<2>::total;
+        case 3: return SignWs<3>::total;
+        case 5: return SignWs<5>::total;
+        default: return 0;
+    }
 }
 
 int launch_sign(int set, uint8_t *pool, size_t pitch, size_t batch, cudaStream_t st, size_t mlen, size_t msg_off,
                 size_t sig_off, size_t scratch_off) {
-    if (batch == 0) return ST_OK;
-    switch (set) {
-        case 1: return sign_t<1>(pool, pitch, batch, st, mlen, msg_off, sig_off, scratch_off);
-        case 2: return sign_t<2>(pool, pitch, batch, st, mlen, msg_off, sig_off, scratch_off);
-        case 3: return sign_t<3>(pool, pitch, batch, st, mlen, msg_off, sig_off, scratch_off);
-        case 5: return sign_t<5>(pool, pitch, batch, st, mlen, msg_off, sig_off, scratch_off);
-        default: return ST_BAD_SET;
-    }
+    SignIO io{pool, pitch, MsgIO{pool + msg_off, pitch, nullptr, nullptr, (uint32_t)mlen},
+              pool + sig_off, pitch, pool + scratch_off, pitch};
+    return launch_sign_io(set, io, batch, st);
 }
 
 }  // namespace mayo

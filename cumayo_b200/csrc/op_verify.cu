@@ -47,8 +47,7 @@ struct VerifyRows {
 __device__ __forceinline__ int pair_index(int i, int j, int k) { return i * k - (i * (i - 1)) / 2 + (j - i); }
 
 template <int SET>
-__global__ void __launch_bounds__(VerifyCfg<SET>::NT) verify_kernel(uint8_t *pool, size_t pitch, uint32_t mlen,
-                                                                     size_t msg_off, size_t sig_off, size_t res_off) {
+__global__ void __launch_bounds__(VerifyCfg<SET>::NT) verify_kernel(const VerifyIO io) {
     using S = Set<SET>;
     using C = VerifyCfg<SET>;
     constexpr int J = C::J, W = C::W, R = C::R, NC = C::NC, NW = C::NW;
@@ -62,9 +61,11 @@ __global__ void __launch_bounds__(VerifyCfg<SET>::NT) verify_kernel(uint8_t *poo
     uint8_t *s_t = smem + C::off_t;
 
     const int tid = threadIdx.x;
-    uint8_t *row = pool + (size_t)blockIdx.x * pitch;
-    const uint8_t *msg = row + msg_off;
-    const uint8_t *sig = row + sig_off;
+    const size_t inst = blockIdx.x;
+    const uint8_t *epk = io.epk + inst * io.epk_stride;
+    const uint8_t *msg = io.m.ptr(inst);
+    const uint32_t mlen = io.m.len(inst);
+    const uint8_t *sig = io.sig + inst * io.sig_stride;
 
     for (int i = tid; i < S::sig; i += C::NT) s_sig[i] = sig[i];
     for (int i = tid; i < J * J * W * 4; i += C::NT) reinterpret_cast<uint32_t *>(xacc)[i] = 0;
@@ -92,7 +93,7 @@ __global__ void __launch_bounds__(VerifyCfg<SET>::NT) verify_kernel(uint8_t *poo
 
         Engine<SET, J, R> eng;
         eng.setup(masks, bs, tid);
-        const VerifyRows<SET> rows{row, row + S::p1, row + S::p};
+        const VerifyRows<SET> rows{epk, epk + S::p1, epk + S::p};
         G4 X[J];
 #pragma unroll
         for (int i = 0; i < J; i++) X[i] = g4_zero();
@@ -147,29 +148,34 @@ __global__ void __launch_bounds__(VerifyCfg<SET>::NT) verify_kernel(uint8_t *poo
             }
         const uint32_t tw = lane < NW ? reinterpret_cast<const uint32_t *>(s_t)[lane] : 0u;
         const bool eq = __all_sync(0xffffffffu, y == tw);
-        if (lane == 0) row[res_off] = eq ? 0 : 1;
+        if (lane == 0) io.res[inst * io.res_stride] = eq ? 0 : 1;
     }
 }
 
 template <int SET>
-static int verify_t(uint8_t *pool, size_t pitch, size_t batch, cudaStream_t st, size_t mlen, size_t msg_off,
-                    size_t sig_off, size_t res_off) {
+static int verify_t(const VerifyIO &io, size_t batch, cudaStream_t st) {
     using C = VerifyCfg<SET>;
     if (!set_smem_attr(verify_kernel<SET>, C::total)) return ST_CUDA;
-    verify_kernel<SET><<<(unsigned)batch, C::NT, C::total, st>>>(pool, pitch, (uint32_t)mlen, msg_off, sig_off, res_off);
+    verify_kernel<SET><<<(unsigned)batch, C::NT, C::total, st>>>(io);
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+int launch_verify_io(int set, const VerifyIO &io, size_t batch, cudaStream_t st) {
+    if (batch == 0) return ST_OK;
+    switch (set) {
+        case 1: return verify_t<1>(io, batch, st);
+        case 2: return verify_t<2>(io, batch, st);
+        case 3: return verify_t<3>(io, batch, st);
+        case 5: return verify_t<5>(io, batch, st);
+        default: return ST_BAD_SET;
+    }
 }
 
 int launch_verify(int set, uint8_t *pool, size_t pitch, size_t batch, cudaStream_t st, size_t mlen, size_t msg_off,
                   size_t sig_off, size_t res_off) {
-    if (batch == 0) return ST_OK;
-    switch (set) {
-        case 1: return verify_t<1>(pool, pitch, batch, st, mlen, msg_off, sig_off, res_off);
-        case 2: return verify_t<2>(pool, pitch, batch, st, mlen, msg_off, sig_off, res_off);
-        case 3: return verify_t<3>(pool, pitch, batch, st, mlen, msg_off, sig_off, res_off);
-        case 5: return verify_t<5>(pool, pitch, batch, st, mlen, msg_off, sig_off, res_off);
-        default: return ST_BAD_SET;
-    }
+    VerifyIO io{pool, pitch, MsgIO{pool + msg_off, pitch, nullptr, nullptr, (uint32_t)mlen}, pool + sig_off, pitch,
+                pool + res_off, pitch};
+    return launch_verify_io(set, io, batch, st);
 }
 
 }  // namespace mayo

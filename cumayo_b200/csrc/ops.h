@@ -34,4 +34,41 @@ int launch_verify(int set, uint8_t *pool, size_t pitch, size_t batch, cudaStream
 int launch_sign(int set, uint8_t *pool, size_t pitch, size_t batch, cudaStream_t st, size_t mlen, size_t msg_off,
                 size_t sig_off, size_t scratch_off);
 
+// Where instance i's operands live.  A stride of 0 on a key shares one key across the batch.
+// Messages are either msg + i*msg_stride with length mlen, or (when msg_off is non-null, a
+// device array) msg + msg_off[i] with length msg_len[i].
+struct MsgIO {
+    const uint8_t *msg;
+    size_t msg_stride;
+    const uint64_t *msg_off;
+    const uint32_t *msg_len;
+    uint32_t mlen;
+#ifdef __CUDACC__
+    __device__ __forceinline__ const uint8_t *ptr(size_t i) const { return msg_off ? msg + msg_off[i] : msg + i * msg_stride; }
+    __device__ __forceinline__ uint32_t len(size_t i) const { return msg_len ? msg_len[i] : mlen; }
+#endif
+};
+struct SignIO {
+    const uint8_t *esk;  // seed_sk || O || P1 || L
+    size_t esk_stride;
+    MsgIO m;
+    uint8_t *sig;
+    size_t sig_stride;
+    uint8_t *ws;  // per-instance workspace of sign_ws_bytes(set) bytes
+    size_t ws_stride;
+};
+struct VerifyIO {
+    const uint8_t *epk;  // P1 || P2 || P3
+    size_t epk_stride;
+    MsgIO m;
+    const uint8_t *sig;
+    size_t sig_stride;
+    uint8_t *res;  // 0 = accept, 1 = reject
+    size_t res_stride;
+};
+int launch_sign_io(int set, const SignIO &io, size_t batch, cudaStream_t st);
+int launch_verify_io(int set, const VerifyIO &io, size_t batch, cudaStream_t st);
+// Workspace bytes per instance used by sign (digest, salt, t, V || r).
+size_t sign_ws_bytes(int set);
+
 }  // namespace mayo

@@ -128,6 +128,24 @@ MAYO_B200_API int mayo_b200_verifyWithepk(int set, uint8_t *pool, size_t mlen, s
 MAYO_B200_API int mayo_b200_verifyWithepk_DtH(int set, uint8_t *result, size_t mlen, const uint8_t *pool,
                                               size_t pitch, size_t batch, void *stream);
 
+/* ---- Extension (no counterpart in the reference API): batched sign/verify over explicit
+ * operand arrays instead of a pool.  Keys may be shared by the whole batch (stride 0, e.g. a
+ * resident expanded key) and messages may have per-instance lengths (the reference takes one
+ * Mlen per call, include/api.cuh:25-47).  All pointers are device pointers.
+ *   message i = msgs + msg_off[i], msg_len[i] bytes    when msg_off != NULL (device arrays)
+ *             = msgs + i * msg_stride, mlen bytes      otherwise
+ * Results are byte-identical to the pool API on the same inputs. */
+/* Per-instance workspace bytes of mayo_b200_sign_many (digest, salt, t, V||r); 0 for a bad set. */
+MAYO_B200_API size_t mayo_b200_sign_ws_bytes(int set);
+MAYO_B200_API int mayo_b200_sign_many(int set, const uint8_t *esk, size_t esk_stride, const uint8_t *msgs,
+                                      const uint64_t *msg_off, const uint32_t *msg_len, size_t msg_stride,
+                                      size_t mlen, uint8_t *sig, size_t sig_stride, uint8_t *ws, size_t batch,
+                                      void *stream);
+MAYO_B200_API int mayo_b200_verify_many(int set, const uint8_t *epk, size_t epk_stride, const uint8_t *msgs,
+                                        const uint64_t *msg_off, const uint32_t *msg_len, size_t msg_stride,
+                                        size_t mlen, const uint8_t *sig, size_t sig_stride, uint8_t *result,
+                                        size_t batch, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -145,3 +145,41 @@ def test_multi_stream_sub_batches(cuda):
     osk, opk = O.keypair_batch(s, 0, sub)
     for i in range(nst):
         assert (sk[i * sub:(i + 1) * sub] == osk).all() and (pk[i * sub:(i + 1) * sub] == opk).all()
+
+
+@pytest.mark.parametrize("s", SETS)
+def test_many_api_shared_key_variable_lengths(s, cuda):
+    """Extension API: one resident expanded key, per-instance message lengths, vs the oracle;
+    also equal to the pool API.  Corrupted signatures must be rejected."""
+    import torch
+    m = Mayo(s)
+    z = m.sizes
+    rng = np.random.default_rng(77 + s)
+    seed = rng.integers(0, 256, (1, z.sk_bytes), dtype=np.uint8)
+    sk, pk = G.keypair_from_seed(m, seed)
+    esk = O.expandsk_batch(s, sk)[0]
+    epk = O.expandpk_batch(s, pk)[0]
+    batch = 40
+    lens = rng.integers(0, 300, batch).astype(np.uint32)
+    msgs = [rng.integers(0, 256, int(n), dtype=np.uint8).tobytes() for n in lens]
+    offs = np.zeros(batch, np.uint64)
+    offs[1:] = np.cumsum(lens[:-1], dtype=np.uint64)
+    d_msgs = torch.from_numpy(np.frombuffer(b"".join(msgs) + b"\0", np.uint8).copy()).cuda()
+    d_offs = torch.from_numpy(offs.view(np.int64)).cuda()
+    d_lens = torch.from_numpy(lens.view(np.int32)).cuda()
+    d_esk = torch.from_numpy(esk.copy()).cuda()
+    d_epk = torch.from_numpy(epk.copy()).cuda()
+    sig = torch.zeros(batch * z.sig_bytes, dtype=torch.uint8, device="cuda")
+    ws = torch.zeros(batch * m.sign_ws_bytes(), dtype=torch.uint8, device="cuda")
+    m.sign_many(d_esk, d_msgs, sig, ws, batch, msg_off=d_offs, msg_len=d_lens)
+    res = torch.full((batch,), 0xEE, dtype=torch.uint8, device="cuda")
+    m.verify_many(d_epk, d_msgs, sig, res, batch, msg_off=d_offs, msg_len=d_lens)
+    torch.cuda.synchronize()
+    osig, _ = O.sign_batch(s, esk[None, :], msgs, shared_key=True)
+    got = sig.cpu().numpy().reshape(batch, z.sig_bytes)
+    assert (got == osig).all()
+    assert res.cpu().numpy().tolist() == [0] * batch
+    bad = torch.from_numpy(G.corrupt(got, 5 + s).reshape(-1)).cuda()
+    m.verify_many(d_epk, d_msgs, bad, res, batch, msg_off=d_offs, msg_len=d_lens)
+    torch.cuda.synchronize()
+    assert res.cpu().numpy().tolist() == [1] * batch
