@@ -490,7 +490,17 @@ def main():
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--int-peak", action="store_true",
+                    help="build and run cumayo_b200/peaks/int_pipes.cu (integer-pipe rates) and exit")
     args = ap.parse_args()
+    if args.int_peak:
+        from cumayo_b200.build import ARCH, BUILD, nvcc
+        os.makedirs(BUILD, exist_ok=True)
+        exe = os.path.join(BUILD, "int_pipes")
+        subprocess.run([nvcc()] + ARCH + ["-O3", "-o", exe, os.path.join(ROOT, "cumayo_b200", "peaks", "int_pipes.cu")],
+                       check=True)
+        subprocess.run([exe], check=True)
+        return
     dist = Dist()
     try:
         out = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
