@@ -90,6 +90,10 @@ def lib() -> ctypes.CDLL:
         L.mayo_b200_sign_many.argtypes = [ctypes.c_int, vp, sz, vp, vp, vp, sz, sz, vp, sz, vp, sz, vp]
         L.mayo_b200_verify_many.restype = ctypes.c_int
         L.mayo_b200_verify_many.argtypes = [ctypes.c_int, vp, sz, vp, vp, vp, sz, sz, vp, sz, vp, sz, vp]
+        L.mayo_b200_sign_noalloc_max_batch.restype = ctypes.c_size_t
+        L.mayo_b200_sign_noalloc_max_batch.argtypes = [ctypes.c_int]
+        L.mayo_b200_sign_many_noalloc.restype = ctypes.c_int
+        L.mayo_b200_sign_many_noalloc.argtypes = [ctypes.c_int, vp, sz, vp, vp, vp, sz, sz, vp, sz, sz, vp]
         _lib = L
     return _lib
 
@@ -287,6 +291,24 @@ class Mayo:
                                            _ptr(msg_len), msg_stride, mlen, _ptr(sig),
                                            z.sig_bytes if sig_stride is None else sig_stride, _ptr(result), batch,
                                            _stream(stream)), "verify_many")
+
+    def sign_noalloc_max_batch(self) -> int:
+        return int(lib().mayo_b200_sign_noalloc_max_batch(self.set))
+
+    def sign_many_noalloc(self, esk, msgs, sig, batch, *, msg_off=None, msg_len=None, msg_stride=0, mlen=0,
+                          esk_stride=0, sig_stride=None, stream=None):
+        """sign_many without a caller workspace, for callers that cannot allocate device memory:
+        the workspace is a fixed array inside the library (batch <= sign_noalloc_max_batch()).
+        Calls must not overlap on the GPU; the first call on a device must precede stream capture."""
+        z = self.sizes
+        rc = lib().mayo_b200_sign_many_noalloc(self.set, _ptr(esk), esk_stride, _ptr(msgs), _ptr(msg_off),
+                                               _ptr(msg_len), msg_stride, mlen, _ptr(sig),
+                                               z.sig_bytes if sig_stride is None else sig_stride, batch,
+                                               _stream(stream))
+        if rc == 4:
+            raise MayoError(f"sign_many_noalloc: batch {batch} exceeds the fixed workspace "
+                            f"(at most {self.sign_noalloc_max_batch()} for MAYO_{self.set})")
+        _check(rc, "sign_many_noalloc")
 
     # pools (the reference benchmark's sizes, tests/bench_stream.cu:25-31, 82, 133) ----------
     def pool_bytes(self, kind: str, mlen: int = 0) -> int:

@@ -119,6 +119,7 @@ MAYO_B200_API const char *mayo_b200_status_string(int status) {
         case MAYO_B200_ERR_SET: return "unknown MAYO parameter set (expected 1, 2, 3 or 5)";
         case MAYO_B200_ERR_ARG: return "invalid argument (null pointer, pitch too small or size out of range)";
         case MAYO_B200_ERR_CUDA: return "CUDA error (see mayo_b200_last_cuda_error)";
+        case MAYO_B200_ERR_TOO_LARGE: return "batch exceeds the fixed workspace of mayo_b200_sign_many_noalloc";
         default: return "unknown status";
     }
 }

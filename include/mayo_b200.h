@@ -39,6 +39,7 @@ typedef enum mayo_b200_status {
     MAYO_B200_ERR_SET = 1,  /* parameter set is not 1, 2, 3 or 5 */
     MAYO_B200_ERR_ARG = 2,  /* null pointer, pitch too small, message too long, ... */
     MAYO_B200_ERR_CUDA = 3, /* a CUDA call failed; see mayo_b200_last_cuda_error() */
+    MAYO_B200_ERR_TOO_LARGE = 4, /* batch exceeds mayo_b200_sign_noalloc_max_batch(set) */
 } mayo_b200_status;
 
 /* Byte sizes of one parameter set (reference include/params.h:10-92 and derived sizes). */
@@ -145,6 +146,22 @@ MAYO_B200_API int mayo_b200_verify_many(int set, const uint8_t *epk, size_t epk_
                                         const uint64_t *msg_off, const uint32_t *msg_len, size_t msg_stride,
                                         size_t mlen, const uint8_t *sig, size_t sig_stride, uint8_t *result,
                                         size_t batch, void *stream);
+
+/* ---- Sign without caller workspace.  No counterpart in the reference API. ----
+ * For callers that cannot allocate device memory (a service whose device-memory budget is
+ * fixed at start-up, or a host program that owns the allocator and forbids a plug-in library
+ * to call cudaMalloc) and so cannot provide the workspace mayo_b200_sign_many needs.  Same
+ * arguments and results as mayo_b200_sign_many minus `ws`: the workspace is a 4 MiB array
+ * compiled into the library, held by every GPU that loads the library until exit.  Batches
+ * above mayo_b200_sign_noalloc_max_batch(set) return MAYO_B200_ERR_TOO_LARGE.  The first call
+ * on a device looks up the array's address on that device: make it before any stream
+ * capture.  All calls share the array, so calls whose GPU work may overlap (different streams
+ * without ordering) race and must not be issued.  Allocates nothing. */
+MAYO_B200_API size_t mayo_b200_sign_noalloc_max_batch(int set);
+MAYO_B200_API int mayo_b200_sign_many_noalloc(int set, const uint8_t *esk, size_t esk_stride, const uint8_t *msgs,
+                                              const uint64_t *msg_off, const uint32_t *msg_len, size_t msg_stride,
+                                              size_t mlen, uint8_t *sig, size_t sig_stride, size_t batch,
+                                              void *stream);
 
 #ifdef __cplusplus
 }
