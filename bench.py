@@ -235,9 +235,138 @@ def run_ours(args, dist: Dist):
         cfg = {"workload": "MAYO_2 shared-key sign+verify", "set": "MAYO_2", "batch": batch,
                "msg_len": "uniform 32..1024 B", "key": "one expanded key resident in HBM",
                "l2": "flushed between steps (256 MiB write)", "api": "mayo_b200_sign_many / verify_many"}
-        check = lambda: int(res.sum().item())  # noqa: E731  (must be 0: every signature accepted)
+        expected = np.zeros(batch, np.uint8)
+        res_dev = lambda: res  # noqa: E731
+    elif wl["kind"] == "keypair_sign_verify":
+        # every instance: seeded keypair -> sign (compact sk, expanded inside) -> verify (compact pk)
+        mlen = wl["mlen"][0]
+        seeds = seeds_for(seed, batch, z.sk_bytes)
+        msgs = chacha((b"mayo-b200-msgs-%d" % seed).ljust(32, b"\0")[:32], batch * mlen).reshape(batch, mlen)
+        kpool, kp = m.alloc_pool("keypair", batch)
+        spool, sp = m.alloc_pool("signWithesk", batch, mlen)
+        vpool, vp = m.alloc_pool("verifyWithepk", batch, mlen)
+        K2, S2, V2 = kpool.view(batch, kp), spool.view(batch, sp), vpool.view(batch, vp)
+        h_seeds = torch.from_numpy(seeds).pin_memory()
+        h_msgs = torch.from_numpy(msgs.copy()).pin_memory()
+        h_pk = torch.zeros((batch, z.pk_bytes), dtype=torch.uint8).pin_memory()
+        h_sig = torch.zeros((batch, z.sig_bytes), dtype=torch.uint8).pin_memory()
+        h_res = torch.zeros(batch, dtype=torch.uint8).pin_memory()
+        pk_off, msg_s, msg_v = A128(z.sk_bytes), A128(z.esk_bytes), A128(z.epk_bytes)
+        sig_s, sig_v = msg_s + A128(mlen), msg_v + A128(mlen)
+        res_off = sig_v + A128(z.sig_bytes)
+        K2[:, : z.sk_bytes].copy_(h_seeds)
+        S2[:, msg_s: msg_s + mlen].copy_(h_msgs)
+        V2[:, msg_v: msg_v + mlen].copy_(h_msgs)
+        launches_per_step = 13  # keypair 4 (hash, AES, tail, P3), signWithesk 6, verifyWithepk 3
+
+        def keypair_op():
+            m.crypto_sign_keypair_from_seed(kpool, kp, batch, st)
+
+        def sign_op():
+            S2[:, : z.sk_bytes].copy_(K2[:, : z.sk_bytes])
+            m.crypto_sign_signWithesk(spool, mlen, sp, batch, st)
+
+        def verify_op():
+            V2[:, z.p_bytes - 16: z.p_bytes - 16 + z.pk_bytes].copy_(K2[:, pk_off: pk_off + z.pk_bytes])
+            V2[:, sig_v: sig_v + z.sig_bytes].copy_(S2[:, sig_s: sig_s + z.sig_bytes])
+            m.crypto_sign_verifyWithepk(vpool, mlen, vp, batch, st)
+
+        def h2d():
+            K2[:, : z.sk_bytes].copy_(h_seeds, non_blocking=True)
+            S2[:, msg_s: msg_s + mlen].copy_(h_msgs, non_blocking=True)
+            V2[:, msg_v: msg_v + mlen].copy_(h_msgs, non_blocking=True)
+
+        def d2h():
+            h_pk.copy_(K2[:, pk_off: pk_off + z.pk_bytes], non_blocking=True)
+            h_sig.copy_(S2[:, sig_s: sig_s + z.sig_bytes], non_blocking=True)
+            h_res.copy_(V2[:, res_off], non_blocking=True)
+
+        h2d_bytes = seeds.nbytes + 2 * msgs.nbytes
+        d2h_bytes = batch * (z.pk_bytes + z.sig_bytes + 1)
+        phases = [("keypair", keypair_op), ("sign", sign_op), ("verify", verify_op)]
+        ops_per_step = 3 * batch
+        macs = mac_counts(s)
+        expand_l = z.m * z.o * z.m * (z.m - 1)  # L = (P1 + P1^T) O + P2 inside signWithesk (v == m)
+        work = {"keypair": macs["keypair"] * batch, "sign": (macs["sign"] + expand_l) * batch,
+                "verify": macs["verify"] * batch}
+        hbm_bytes = {"keypair": 2 * batch * z.p_bytes, "sign": 3 * batch * z.esk_bytes,
+                     "verify": 2 * batch * z.epk_bytes}
+        cfg = {"workload": "MAYO_1 keypair -> sign -> verify, distinct keys", "set": f"MAYO_{s}", "batch": batch,
+               "msg_len": f"{mlen} B", "key": "per-instance seeded keypairs (ChaCha20)",
+               "l2": "flushed between steps (256 MiB write)",
+               "api": "crypto_sign_keypair_from_seed / signWithesk / verifyWithepk (pool API)"}
+        expected = np.zeros(batch, np.uint8)
+        res_dev = lambda: V2[:, res_off]  # noqa: E731
+    elif wl["kind"] == "distinct_verify":
+        # every instance has its own keypair; epk resident in the verify pool, 10% corrupted sigs
+        mlen = wl["mlen"][0]
+        seeds = seeds_for(seed, batch, z.sk_bytes)
+        msgs = chacha((b"mayo-b200-msgs-%d" % seed).ljust(32, b"\0")[:32], batch * mlen).reshape(batch, mlen)
+        vpool, vp = m.alloc_pool("verify", batch, mlen)
+        V2 = vpool.view(batch, vp)
+        msg_v = A128(z.epk_bytes)
+        sig_v = msg_v + A128(mlen)
+        res_off = sig_v + A128(z.sig_bytes)
+        chunk = 2048  # set-up in chunks: keypair pools are large for MAYO_5
+        for c0 in range(0, batch, chunk):
+            nb = min(chunk, batch - c0)
+            kpool, kp = m.alloc_pool("keypair", nb)
+            K2 = kpool.view(nb, kp)
+            K2[:, : z.sk_bytes].copy_(torch.from_numpy(seeds[c0:c0 + nb]))
+            m.crypto_sign_keypair_from_seed(kpool, kp, nb, st)
+            pk_off = A128(z.sk_bytes)
+            V2[c0:c0 + nb, z.p_bytes - 16: z.p_bytes - 16 + z.pk_bytes].copy_(K2[:, pk_off: pk_off + z.pk_bytes])
+            spool, spch = m.alloc_pool("signWithesk", nb, mlen)
+            S2 = spool.view(nb, spch)
+            S2[:, : z.sk_bytes].copy_(K2[:, : z.sk_bytes])
+            ms_ = A128(z.esk_bytes)
+            S2[:, ms_: ms_ + mlen].copy_(torch.from_numpy(msgs[c0:c0 + nb]))
+            m.crypto_sign_signWithesk(spool, mlen, spch, nb, st)
+            ss_ = ms_ + A128(mlen)
+            V2[c0:c0 + nb, sig_v: sig_v + z.sig_bytes].copy_(S2[:, ss_: ss_ + z.sig_bytes])
+            del kpool, spool
+        m.crypto_sign_expandpk(vpool, vp, batch, st)
+        V2[:, msg_v: msg_v + mlen].copy_(torch.from_numpy(msgs))
+        torch.cuda.synchronize()
+        good_sigs = V2[:, sig_v: sig_v + z.sig_bytes].cpu().numpy()
+        rng = np.random.default_rng(seed)
+        bad_idx = np.sort(rng.choice(batch, batch // 10, replace=False))
+        sigs = good_sigs.copy()
+        for i in bad_idx:
+            pos = int(rng.integers(0, 2 * z.sig_bytes))
+            sigs[i, pos // 2] ^= np.uint8(int(rng.integers(1, 16)) << (4 * (pos % 2)))
+        h_sig = torch.from_numpy(sigs).pin_memory()
+        h_msgs = torch.from_numpy(msgs.copy()).pin_memory()
+        h_res = torch.zeros(batch, dtype=torch.uint8).pin_memory()
+        V2[:, sig_v: sig_v + z.sig_bytes].copy_(h_sig)
+        launches_per_step = 1
+
+        def verify_op():
+            m.crypto_sign_verify(vpool, mlen, vp, batch, st)
+
+        def h2d():
+            V2[:, msg_v: msg_v + mlen].copy_(h_msgs, non_blocking=True)
+            V2[:, sig_v: sig_v + z.sig_bytes].copy_(h_sig, non_blocking=True)
+
+        def d2h():
+            h_res.copy_(V2[:, res_off], non_blocking=True)
+
+        h2d_bytes = msgs.nbytes + sigs.nbytes
+        d2h_bytes = batch
+        phases = [("verify", verify_op)]
+        ops_per_step = batch
+        work = {"verify": mac_counts(s)["verify"] * batch}
+        hbm_bytes = {"verify": batch * (z.epk_bytes + z.sig_bytes + mlen)}
+        cfg = {"workload": f"MAYO_{s} distinct-key verify", "set": f"MAYO_{s}", "batch": batch,
+               "msg_len": f"{mlen} B", "key": "per-instance expanded public keys resident in HBM (pool rows)",
+               "corrupted": "10% (one random nibble flipped), must return 1",
+               "l2": "inputs larger than L2 (EPKs) and flushed between steps",
+               "api": "crypto_sign_verify (pool API)"}
+        expected = np.zeros(batch, np.uint8)
+        expected[bad_idx] = 1
+        res_dev = lambda: V2[:, res_off]  # noqa: E731
     else:
-        raise SystemExit(f"workload {args.workload} not implemented in this arm yet")
+        raise SystemExit(f"unknown workload {args.workload}")
 
     def step():
         flush.fill_(1)
@@ -247,7 +376,7 @@ def run_ours(args, dist: Dist):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    bad = check()
+    bad = int((res_dev().cpu().numpy() != expected).sum())
 
     # ---- device-resident timing ----
     ev = {name: [] for name, _ in phases}
@@ -287,7 +416,7 @@ def run_ours(args, dist: Dist):
     e1.record(st)
     torch.cuda.synchronize()
     e2e_ms = dist.max(e0.elapsed_time(e1))
-    bad_e2e = int(h_res.sum().item())
+    bad_e2e = int((h_res.numpy() != expected).sum())
 
     ms_per_step = total_ms / args.steps
     value = ops_per_step * dist.world / (ms_per_step / 1e3)
@@ -303,20 +432,26 @@ def run_ours(args, dist: Dist):
         "sign_per_s": round(batch * dist.world / (phase_ms["sign"] / 1e3), 1) if "sign" in phase_ms else None,
         "verify_per_s": round(batch * dist.world / (phase_ms["verify"] / 1e3), 1) if "verify" in phase_ms else None,
         "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
-        "roofline": {"bound": "alu", "kernel": f"{dom} ({args.workload})", "achieved": round(ach_ops, 1),
-                     "peak": round(peak_ops, 1), "unit": "G int-ops/s", "frac": round(ach_ops / peak_ops, 4),
-                     "traffic": None,
-                     "definition": "algorithmic ops = 0.5 x GF(16) MACs (16 LOP3 per 32 MACs); peak = measured "
-                                   "LOP3 issue rate 64 lane-ops/clk/SM x 148 SMs x median SM clock"},
-        "roofline_hbm": {"bound": "hbm", "achieved": round(hbm_bytes[dom] / (phase_ms[dom] / 1e3) / 1e9, 2),
+        "roofline_alu": {"bound": "alu", "kernel": f"{dom} ({args.workload})", "achieved": round(ach_ops, 1),
+                         "peak": round(peak_ops, 1), "unit": "G int-ops/s", "frac": round(ach_ops / peak_ops, 4),
+                         "traffic": None,
+                         "definition": "algorithmic ops = 0.5 x GF(16) MACs (16 LOP3 per 32 MACs); peak = measured "
+                                       "LOP3 issue rate 64 lane-ops/clk/SM x 148 SMs x median SM clock"},
+        "roofline_hbm": {"bound": "hbm", "kernel": f"{dom} ({args.workload})",
+                         "achieved": round(hbm_bytes[dom] / (phase_ms[dom] / 1e3) / 1e9, 2),
                          "peak": 6550.1, "unit": "GB/s",
-                         "frac": round(hbm_bytes[dom] / (phase_ms[dom] / 1e3) / 1e9 / 6550.1, 5)},
+                         "frac": round(hbm_bytes[dom] / (phase_ms[dom] / 1e3) / 1e9 / 6550.1, 5), "traffic": None,
+                         "definition": "algorithmic bytes the kernel must move from HBM per launch / kernel time; "
+                                       "peak = MEASURED_PEAKS hbm_gbs (copy)"},
         "e2e": {"value": round(ops_per_step * dist.world / (e2e_ms / args.steps / 1e3), 1), "unit": "ops/s",
                 "h2d_bytes_per_step": int(h2d_bytes), "d2h_bytes_per_step": int(d2h_bytes)},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk,
-        "rejected_valid_signatures": bad + bad_e2e,
+        "result_mismatches": bad + bad_e2e,
     }
+    # The binding roof: distinct-key verify streams every EPK from HBM (bound hbm); the other
+    # workloads keep keys L2-resident and are integer-ALU bound (bound alu).
+    out["roofline"] = dict(out["roofline_hbm"] if wl["kind"] == "distinct_verify" else out["roofline_alu"])
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
     return out
@@ -350,6 +485,39 @@ def cpu_baseline(args, sample: int | None = None):
                 "sample": f"{sample} signs + {sample} verifies of the same workload (shared MAYO_2 key, "
                           f"32..1024 B messages), OpenMP one instance per thread",
                 "sign_per_s": round(sample / t_sign, 1), "verify_per_s": round(sample / t_ver, 1)}
+    if wl["kind"] == "keypair_sign_verify":
+        sample = sample or 4 * wl["batch"]
+        seeds = seeds_for(1, sample, P.sk_bytes)
+        msgs = chacha(b"mayo-b200-msgs-1".ljust(32, b"\0"), sample * 32).reshape(sample, 32)
+        t = time.perf_counter()
+        pk = O.keypair_from_seed_batch(s, seeds)
+        t_kp = time.perf_counter() - t
+        t = time.perf_counter()
+        sig, _ = O.sign_batch(s, O.expandsk_batch(s, seeds), [bytes(x) for x in msgs])
+        t_sign = time.perf_counter() - t
+        t = time.perf_counter()
+        res = O.verify_batch(s, O.expandpk_batch(s, pk), [bytes(x) for x in msgs], sig)
+        t_ver = time.perf_counter() - t
+        assert int(res.sum()) == 0
+        return {"value": round(3 * sample / (t_kp + t_sign + t_ver), 1), "unit": "ops/s", "cores": threads,
+                "kind": "port", "sample": f"{sample} instances of keypair -> sign (expand-sk inside) -> verify "
+                                          f"(expand-pk inside), MAYO_{s}, OpenMP one instance per thread",
+                "keypair_per_s": round(sample / t_kp, 1), "sign_per_s": round(sample / t_sign, 1),
+                "verify_per_s": round(sample / t_ver, 1)}
+    if wl["kind"] == "distinct_verify":
+        sample = sample or (512 if s == 5 else 1024)
+        seeds = seeds_for(1, sample, P.sk_bytes)
+        msgs = [bytes(x) for x in chacha(b"mayo-b200-msgs-1".ljust(32, b"\0"), sample * 32).reshape(sample, 32)]
+        pk = O.keypair_from_seed_batch(s, seeds)
+        sig, _ = O.sign_batch(s, O.expandsk_batch(s, seeds), msgs)
+        epk = O.expandpk_batch(s, pk)
+        t = time.perf_counter()
+        res = O.verify_batch(s, epk, msgs, sig)
+        t_ver = time.perf_counter() - t
+        assert int(res.sum()) == 0
+        return {"value": round(sample / t_ver, 1), "unit": "ops/s", "cores": threads, "kind": "port",
+                "sample": f"{sample} distinct-key verifies (expanded keys precomputed), MAYO_{s}, OpenMP one "
+                          f"instance per thread"}
     return None
 
 
@@ -366,7 +534,7 @@ def run_reference(args, dist: Dist):
     if not os.path.exists(path):
         return {"impl": "reference", "unavailable": f"{path} not built (make -C oracle ref needs the reference sources)"}
     if wl["kind"] != "shared_sign_verify":
-        return {"impl": "reference", "unavailable": f"reference arm for {args.workload} not implemented"}
+        return run_reference_pool(args, dist, path)
     L = ctypes.CDLL(path)
     vp, sz = ctypes.c_void_p, ctypes.c_size_t
     for f in ("ref_sign", "ref_verify"):
@@ -479,6 +647,136 @@ def run_reference(args, dist: Dist):
                              "sample": "not a CPU run: the reference has no CPU implementation; this arm times "
                                        "its own CUDA build on the same B200"},
             "e2e": {"value": round(value, 1), "unit": "ops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def _ref_lib(path):
+    import ctypes
+    L = ctypes.CDLL(path)
+    vp, sz = ctypes.c_void_p, ctypes.c_size_t
+    L.ref_keypair.argtypes = [vp, sz, sz, vp, sz]
+    for f in ("ref_expandsk", "ref_expandpk"):
+        getattr(L, f).argtypes = [vp, sz, sz, vp]
+    for f in ("ref_sign", "ref_signWithesk", "ref_verify", "ref_verifyWithepk"):
+        getattr(L, f).argtypes = [vp, sz, sz, sz, vp]
+    L.ref_init()
+    return L
+
+
+def run_reference_pool(args, dist: Dist, path: str):
+    """c1 and c3 on the reference's own build, pool API only (the reference generates its keys
+    with its counter seeds, since its API takes no caller seed; the work is the same)."""
+    import torch
+    wl = WORKLOADS[args.workload]
+    s, batch = wl["set"], args.batch or wl["batch"]
+    from oracle import oracle as O
+    P = O.params(s)
+    L = _ref_lib(path)
+    torch.cuda.set_device(dist.local)
+    dev = torch.device("cuda", dist.local)
+    cur = torch.cuda.current_stream()
+    sptr = cur.cuda_stream
+    mlen = wl["mlen"][0]
+    rup = lambda x: (x + 511) // 512 * 512  # noqa: E731
+    kp = rup(A128(P.sk_bytes) + A128(P.pk_bytes) + A128(P.p_bytes))
+    sp = rup(A128(P.esk_bytes) + A128(mlen) + A128(P.sig_bytes) + A128(P.k * P.m * ((P.o + 1) // 2)))
+    vp = rup(A128(P.epk_bytes) + A128(mlen) + A128(P.sig_bytes) + 1)
+    pk_off, msg_s, msg_v = A128(P.sk_bytes), A128(P.esk_bytes), A128(P.epk_bytes)
+    sig_s, sig_v = msg_s + A128(mlen), msg_v + A128(mlen)
+    res_off = sig_v + A128(P.sig_bytes)
+    msgs = torch.from_numpy(chacha(b"mayo-b200-msgs-1".ljust(32, b"\0"), batch * mlen).reshape(batch, mlen).copy())
+
+    def ev_time(fn) -> float:
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(cur)
+        fn()
+        b.record(cur)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    if wl["kind"] == "keypair_sign_verify":
+        K = torch.zeros((batch, kp), dtype=torch.uint8, device=dev)
+        S = torch.zeros((batch, sp), dtype=torch.uint8, device=dev)
+        V = torch.zeros((batch, vp), dtype=torch.uint8, device=dev)
+        S[:, msg_s: msg_s + mlen].copy_(msgs)
+        V[:, msg_v: msg_v + mlen].copy_(msgs)
+
+        def kp_op():
+            L.ref_keypair(K.data_ptr(), kp, batch, sptr, 0)
+
+        def sign_op():
+            S[:, : P.sk_bytes].copy_(K[:, : P.sk_bytes])
+            L.ref_signWithesk(S.data_ptr(), mlen, sp, batch, sptr)
+
+        def verify_op():
+            V[:, P.p_bytes - 16: P.p_bytes - 16 + P.pk_bytes].copy_(K[:, pk_off: pk_off + P.pk_bytes])
+            V[:, sig_v: sig_v + P.sig_bytes].copy_(S[:, sig_s: sig_s + P.sig_bytes])
+            L.ref_verifyWithepk(V.data_ptr(), mlen, vp, batch, sptr)
+
+        phases = [("keypair", kp_op), ("sign", sign_op), ("verify", verify_op)]
+        ops = 3 * batch
+        expected = np.zeros(batch, np.uint8)
+        cfg = {"workload": f"MAYO_{s} keypair -> sign -> verify, distinct keys", "set": f"MAYO_{s}",
+               "batch": batch, "msg_len": f"{mlen} B",
+               "api": "crypto_sign_keypair / signWithesk / verifyWithepk (counter-seeded keys)"}
+    else:
+        V = torch.zeros((batch, vp), dtype=torch.uint8, device=dev)
+        chunk = 2048
+        for c0 in range(0, batch, chunk):
+            nb = min(chunk, batch - c0)
+            K = torch.zeros((nb, kp), dtype=torch.uint8, device=dev)
+            L.ref_keypair(K.data_ptr(), kp, nb, sptr, 2 * c0)
+            S = torch.zeros((nb, sp), dtype=torch.uint8, device=dev)
+            S[:, : P.sk_bytes].copy_(K[:, : P.sk_bytes])
+            S[:, msg_s: msg_s + mlen].copy_(msgs[c0:c0 + nb])
+            L.ref_signWithesk(S.data_ptr(), mlen, sp, nb, sptr)
+            V[c0:c0 + nb, P.p_bytes - 16: P.p_bytes - 16 + P.pk_bytes].copy_(K[:, pk_off: pk_off + P.pk_bytes])
+            V[c0:c0 + nb, sig_v: sig_v + P.sig_bytes].copy_(S[:, sig_s: sig_s + P.sig_bytes])
+            del K, S
+        L.ref_expandpk(V.data_ptr(), vp, batch, sptr)
+        V[:, msg_v: msg_v + mlen].copy_(msgs)
+        torch.cuda.synchronize()
+        sig = V[:, sig_v: sig_v + P.sig_bytes].cpu().numpy()
+        rng = np.random.default_rng(1)
+        bad_idx = np.sort(rng.choice(batch, batch // 10, replace=False))
+        for i in bad_idx:
+            pos = int(rng.integers(0, 2 * P.sig_bytes))
+            sig[i, pos // 2] ^= np.uint8(int(rng.integers(1, 16)) << (4 * (pos % 2)))
+        V[:, sig_v: sig_v + P.sig_bytes].copy_(torch.from_numpy(sig))
+        expected = np.zeros(batch, np.uint8)
+        expected[bad_idx] = 1
+
+        def verify_op():
+            L.ref_verify(V.data_ptr(), mlen, vp, batch, sptr)
+
+        phases = [("verify", verify_op)]
+        ops = batch
+        cfg = {"workload": f"MAYO_{s} distinct-key verify", "set": f"MAYO_{s}", "batch": batch,
+               "msg_len": f"{mlen} B", "corrupted": "10%", "api": "crypto_sign_verify (epk resident in the pool)"}
+    for _ in range(args.warmup):
+        for _, fn in phases:
+            fn()
+    torch.cuda.synchronize()
+    dist.barrier()
+    per = {name: 0.0 for name, _ in phases}
+    for _ in range(args.steps):
+        for name, fn in phases:
+            per[name] += ev_time(fn)
+    dist.barrier()
+    mism = int((V[:, res_off].cpu().numpy() != expected).sum())
+    ms = dist.max(sum(per.values()) / args.steps)
+    value = ops * dist.world / (ms / 1e3)
+    out = {"metric": METRIC, "value": round(value, 1), "unit": "ops/s", "impl": "reference", "n_gpus": dist.world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded ChaCha20 messages)",
+           "config": cfg, "phase_ms": {k: round(v / args.steps, 3) for k, v in per.items()},
+           "result_mismatches": mism,
+           "cpu_baseline": {"value": round(value, 1), "unit": "ops/s", "cores": 0, "kind": "reference",
+                            "sample": "not a CPU run: the reference has no CPU implementation; this arm times its "
+                                      "own CUDA build on the same B200"},
+           "e2e": {"value": round(value, 1), "unit": "ops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    for name in per:
+        out[f"{name}_per_s"] = round(batch * dist.world / (per[name] / args.steps / 1e3), 1)
+    return out
 
 
 def main():

@@ -96,7 +96,7 @@ struct SignCfg {
     static constexpr size_t off_upk = off_x + (size_t)J * J * W * 16;
     static constexpr size_t off_mpk = off_upk + pad16((size_t)S::pairs * NW * 4);
     static constexpr size_t off_piv = off_mpk + pad16((size_t)S::k * S::o * NW * 4);
-    static constexpr size_t off_rhs = off_piv + (size_t)2 * W * 16;
+    static constexpr size_t off_rhs = off_piv + (size_t)2 * (W + 2) * 16;
     static constexpr size_t off_y = off_rhs + (size_t)W * 16;
     static constexpr size_t off_key = off_y + pad16(NW * 4);
     static constexpr size_t off_t = off_key + pad16(S::digest + 2 * S::sk + 1);
@@ -395,43 +395,54 @@ __global__ void __launch_bounds__(SignCfg<SET>::NT) sign_kernel(const SignIO io)
         }
 #pragma unroll 1
         for (int pc = 0; pc < KO; pc++) {
-            uint4 *buf = pivbuf + (pc & 1) * W;
+            // The owner of column pc computes the pivot (lowest unpivoted row with a nonzero
+            // entry), its inverse and F' = inv * (a + e_p), and publishes F' and the row one-hot.
+            uint4 *buf = pivbuf + (pc & 1) * (W + 2);
+            uint32_t *ohw = reinterpret_cast<uint32_t *>(buf + W);  // oh[0..W), found at [7]
 #pragma unroll
-            for (int q = 0; q < CPT; q++)
-                if (tid + NT * q == pc)
+            for (int q = 0; q < CPT; q++) {
+                if (tid + NT * q != pc) continue;
+                uint32_t oh[W], found = 0;
 #pragma unroll
-                    for (int w = 0; w < W; w++) g4_st(buf + w, col[q][w]);
+                for (int w = 0; w < W; w++) {
+                    const G4 &a = col[q][w];
+                    const uint32_t nz = (a.p0 | a.p1 | a.p2 | a.p3) & ~pivoted[w];
+                    const uint32_t low = nz & (0u - nz);
+                    oh[w] = low & ~found;
+                    found |= 0u - (uint32_t)(nz != 0u);
+                }
+                uint32_t o0 = 0, o1 = 0, o2 = 0, o3 = 0;
+#pragma unroll
+                for (int w = 0; w < W; w++) {
+                    o0 |= col[q][w].p0 & oh[w];
+                    o1 |= col[q][w].p1 & oh[w];
+                    o2 |= col[q][w].p2 & oh[w];
+                    o3 |= col[q][w].p3 & oh[w];
+                }
+                const uint32_t piv = (uint32_t)(o0 != 0) | ((uint32_t)(o1 != 0) << 1) |
+                                     ((uint32_t)(o2 != 0) << 2) | ((uint32_t)(o3 != 0) << 3);
+                const uint4 inv_m = scalar_masks(gf16_inv_ct(piv) & found);
+#pragma unroll
+                for (int w = 0; w < W; w++) {
+                    G4 ap = col[q][w];
+                    ap.p0 ^= oh[w];
+                    G4 F = g4_zero();
+                    g4_madd(F, ap, inv_m);
+                    g4_st(buf + w, F);
+                    ohw[w] = oh[w];
+                    my_oh[q][w] = oh[w];
+                }
+                ohw[7] = found;
+                my_has[q] = found;
+            }
             __syncthreads();
-            G4 a[W];
-            uint32_t oh[W], found = 0;
-#pragma unroll
-            for (int w = 0; w < W; w++) {
-                a[w] = g4_ld(buf + w);
-                const uint32_t nz = (a[w].p0 | a[w].p1 | a[w].p2 | a[w].p3) & ~pivoted[w];
-                const uint32_t low = nz & (0u - nz);
-                oh[w] = low & ~found;
-                found |= 0u - (uint32_t)(nz != 0u);
-            }
-            // pivot value a[p] and its inverse (0 when the column has no pivot)
-            uint32_t o0 = 0, o1 = 0, o2 = 0, o3 = 0;
-#pragma unroll
-            for (int w = 0; w < W; w++) {
-                o0 |= a[w].p0 & oh[w];
-                o1 |= a[w].p1 & oh[w];
-                o2 |= a[w].p2 & oh[w];
-                o3 |= a[w].p3 & oh[w];
-            }
-            const uint32_t piv = (uint32_t)(o0 != 0) | ((uint32_t)(o1 != 0) << 1) | ((uint32_t)(o2 != 0) << 2) |
-                                 ((uint32_t)(o3 != 0) << 3);
-            const uint4 inv_m = scalar_masks(gf16_inv_ct(piv) & found);
-            // F' = inv * (a + e_p): eliminates every other row and normalises row p
+            // every column: col ^= col[p] * F'  (eliminates row p elsewhere, normalises row p)
             G4 F[W];
+            uint32_t oh[W];
 #pragma unroll
             for (int w = 0; w < W; w++) {
-                G4 ap = a[w];
-                ap.p0 ^= oh[w];
-                F[w] = g4_zero();
-                g4_madd(F[w], ap, inv_m);
+                F[w] = g4_ld(buf + w);
+                oh[w] = ohw[w];
             }
 #pragma unroll
             for (int q = 0; q < CPT; q++) {
@@ -448,11 +459,6 @@ __global__ void __launch_bounds__(SignCfg<SET>::NT) sign_kernel(const SignIO io)
                 const uint4 em = scalar_masks(ev);
 #pragma unroll
                 for (int w = 0; w < W; w++) g4_madd(col[q][w], F[w], em);
-                if (tid + NT * q == pc) {
-#pragma unroll
-                    for (int w = 0; w < W; w++) my_oh[q][w] = oh[w];
-                    my_has[q] = found;
-                }
             }
 #pragma unroll
             for (int w = 0; w < W; w++) pivoted[w] |= oh[w];
@@ -467,7 +473,7 @@ __global__ void __launch_bounds__(SignCfg<SET>::NT) sign_kernel(const SignIO io)
         for (int q = 0; q < CPT; q++)
             if (tid + NT * q == KO)
 #pragma unroll
-                for (int w = 0; w < W; w++) g4_st(pivbuf + w, col[q][w]);
+                for (int w = 0; w < W; w++) g4_st(rhsacc + w, col[q][w]);  // not a buffer still being read
         __syncthreads();
 #pragma unroll
         for (int q = 0; q < CPT; q++) {
@@ -476,7 +482,7 @@ __global__ void __launch_bounds__(SignCfg<SET>::NT) sign_kernel(const SignIO io)
                 uint32_t z0 = 0, z1 = 0, z2 = 0, z3 = 0;
 #pragma unroll
                 for (int w = 0; w < W; w++) {
-                    const G4 h = g4_ld(pivbuf + w);
+                    const G4 h = g4_ld(rhsacc + w);
                     z0 |= h.p0 & my_oh[q][w];
                     z1 |= h.p1 & my_oh[q][w];
                     z2 |= h.p2 & my_oh[q][w];
