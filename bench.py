@@ -43,6 +43,7 @@ WORKLOADS = {
     "c1": dict(set=1, batch=1024, kind="keypair_sign_verify", mlen=(32, 32)),
     "c3-3": dict(set=3, batch=16384, kind="distinct_verify", mlen=(32, 32)),
     "c3-5": dict(set=5, batch=16384, kind="distinct_verify", mlen=(32, 32)),
+    "c4": dict(set=0, batch=262144, kind="mixed_queue", mlen=(32, 32)),
 }
 
 PARAMS = {1: (86, 78, 8, 10), 2: (81, 64, 17, 4), 3: (118, 108, 10, 11), 5: (154, 142, 12, 12)}
@@ -131,7 +132,7 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
@@ -173,7 +174,7 @@ def run_ours(args, dist: Dist):
 
     wl = WORKLOADS[args.workload]
     s, batch = wl["set"], args.batch or wl["batch"]
-    m = M.Mayo(s)
+    m = M.Mayo(s if s else 1)
     z = m.sizes
     dev = torch.device("cuda", dist.local)
     torch.cuda.set_device(dev)
@@ -181,6 +182,7 @@ def run_ours(args, dist: Dist):
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     launches_per_step = 0
     seed = 1 + dist.rank
+    plain_fn = None
 
     if wl["kind"] == "shared_sign_verify":
         # one resident expanded key (esk, epk), messages of per-instance length
@@ -365,6 +367,9 @@ def run_ours(args, dist: Dist):
         expected = np.zeros(batch, np.uint8)
         expected[bad_idx] = 1
         res_dev = lambda: V2[:, res_off]  # noqa: E731
+    elif wl["kind"] == "mixed_queue":
+        phases, h2d, d2h, h2d_bytes, d2h_bytes, ops_per_step, work, hbm_bytes, cfg, expected, res_dev, h_res, \
+            plain_fn, launches_per_step = setup_mixed_queue(args, dist, batch, seed, st)
     else:
         raise SystemExit(f"unknown workload {args.workload}")
 
@@ -398,11 +403,10 @@ def run_ours(args, dist: Dist):
     t1.record(st)
     torch.cuda.synchronize()
     dist.barrier()
-    clk = clocks.stop()
     total_ms = dist.max(t0.elapsed_time(t1))
     phase_ms = {name: sum(a.elapsed_time(b) for a, b in lst) / len(lst) for name, lst in ev.items()}
 
-    # ---- end to end through the public API with host buffers ----
+    # ---- end to end through the public API with host buffers (clocks keep sampling) ----
     dist.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -415,6 +419,7 @@ def run_ours(args, dist: Dist):
         d2h()
     e1.record(st)
     torch.cuda.synchronize()
+    clk = clocks.stop()
     e2e_ms = dist.max(e0.elapsed_time(e1))
     bad_e2e = int((h_res.numpy() != expected).sum())
 
@@ -452,9 +457,145 @@ def run_ours(args, dist: Dist):
     # The binding roof: distinct-key verify streams every EPK from HBM (bound hbm); the other
     # workloads keep keys L2-resident and are integer-ALU bound (bound alu).
     out["roofline"] = dict(out["roofline_hbm"] if wl["kind"] == "distinct_verify" else out["roofline_alu"])
+    if plain_fn is not None:
+        # the same work as per-(set, op) batched launches on the same GPU
+        for _ in range(args.warmup):
+            plain_fn()
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(st)
+        for _ in range(args.steps):
+            flush.fill_(1)
+            plain_fn()
+        p1.record(st)
+        torch.cuda.synchronize()
+        plain_ms = dist.max(p0.elapsed_time(p1)) / args.steps
+        out["plain"] = {"value": round(ops_per_step * dist.world / (plain_ms / 1e3), 1), "ms_per_step": round(plain_ms, 4),
+                        "api": "per-(set, op) batched launches: keypair_from_seed, sign_many, verify_many"}
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
     return out
+
+
+def expand_shared_key(m, key_seed: np.ndarray, dev, st):
+    """(esk, epk) device tensors for one caller-seeded keypair, through the pool API."""
+    import torch
+    z = m.sizes
+    kp, kpitch = m.alloc_pool("keypair", 1)
+    kp[: z.sk_bytes].copy_(torch.from_numpy(key_seed))
+    m.crypto_sign_keypair_from_seed(kp, kpitch, 1, st)
+    esk = torch.zeros(z.esk_bytes, dtype=torch.uint8, device=dev)
+    esk[: z.sk_bytes].copy_(kp[: z.sk_bytes])
+    m.crypto_sign_expandsk(esk, z.esk_bytes, 1, st)
+    epk = torch.zeros(z.epk_bytes, dtype=torch.uint8, device=dev)
+    pk_off = A128(z.sk_bytes)
+    epk[z.p_bytes - 16: z.p_bytes - 16 + z.pk_bytes].copy_(kp[pk_off: pk_off + z.pk_bytes])
+    m.crypto_sign_expandpk(epk, z.epk_bytes, 1, st)
+    return esk, epk
+
+
+def setup_mixed_queue(args, dist, batch, seed, st):
+    """C4: `batch` operations uniform over {MAYO_1,2,3,5} x {keypair, sign, verify}, shuffled, in
+    one persistent queue launch replayed from a CUDA graph; shape chosen by the autotuner.  The
+    same work as per-(set, op) batched launches is the comparison (`plain`)."""
+    import torch
+
+    import cumayo_b200 as M
+    from cumayo_b200 import autotune as AT
+    from cumayo_b200 import queue as Q
+    dev = torch.cuda.current_device()
+    sets, mlen = [1, 2, 3, 5], 32
+    per = [batch // 12 + (1 if i < batch % 12 else 0) for i in range(12)]
+    operands, entries, plain_parts = {}, [], []
+    h2d_list, d2h_list, h_res_parts = [], [], []
+    work_macs = 0.0
+    for si, s in enumerate(sets):
+        m = M.Mayo(s)
+        z = m.sizes
+        n_kp, n_sg, n_vf = per[3 * si], per[3 * si + 1], per[3 * si + 2]
+        seeds = seeds_for(seed * 10 + s, n_kp, z.sk_bytes)
+        esk, epk = expand_shared_key(m, seeds_for(seed * 10 + s + 5, 1, z.sk_bytes)[0], dev, st)
+        msg_sg = chacha((b"c4-sign-%d-%d" % (seed, s)).ljust(32, b"\0"), n_sg * mlen).reshape(n_sg, mlen)
+        msg_vf = chacha((b"c4-verify-%d-%d" % (seed, s)).ljust(32, b"\0"), n_vf * mlen).reshape(n_vf, mlen)
+        d_seeds = torch.from_numpy(seeds).to(dev)
+        d_pk = torch.zeros(n_kp * z.pk_bytes, dtype=torch.uint8, device=dev)
+        d_msg_sg = torch.from_numpy(msg_sg.copy()).to(dev)
+        d_sig_sg = torch.zeros(n_sg * z.sig_bytes, dtype=torch.uint8, device=dev)
+        d_msg_vf = torch.from_numpy(msg_vf.copy()).to(dev)
+        d_sig_vf = torch.zeros(n_vf * z.sig_bytes, dtype=torch.uint8, device=dev)
+        d_res = torch.full((n_vf,), 0xEE, dtype=torch.uint8, device=dev)
+        ws = torch.zeros(max(n_sg, n_vf) * m.sign_ws_bytes(), dtype=torch.uint8, device=dev)
+        m.sign_many(esk, d_msg_vf, d_sig_vf, ws, n_vf, msg_stride=mlen, mlen=mlen, stream=st)  # valid signatures
+        operands[s] = Q.SetOperands(kp_seed=d_seeds, kp_pk=d_pk, sg_esk=esk, sg_nkeys=1, sg_msg=d_msg_sg,
+                                    sg_mlen=mlen, sg_sig=d_sig_sg, vf_epk=epk, vf_nkeys=1, vf_msg=d_msg_vf,
+                                    vf_mlen=mlen, vf_sig=d_sig_vf, vf_res=d_res)
+        entries += [(Q.OP_KEYPAIR, s, i) for i in range(n_kp)] + [(Q.OP_SIGN, s, i) for i in range(n_sg)] + \
+                   [(Q.OP_VERIFY, s, i) for i in range(n_vf)]
+        mc = mac_counts(s)
+        work_macs += n_kp * mc["keypair"] + n_sg * mc["sign"] + n_vf * mc["verify"]
+        # plain per-(set, op) launches doing the same work
+        kpool, kpch = m.alloc_pool("keypair", n_kp)
+        kpool.view(n_kp, kpch)[:, : z.sk_bytes].copy_(d_seeds)
+        plain_parts.append((m, kpool, kpch, n_kp, esk, epk, d_msg_sg, d_sig_sg, n_sg, d_msg_vf, d_sig_vf,
+                            d_res, n_vf, ws))
+        h_seeds = torch.from_numpy(seeds).pin_memory()
+        h_msgs = torch.from_numpy(msg_sg.copy()).pin_memory()
+        h_msgv = torch.from_numpy(msg_vf.copy()).pin_memory()
+        h_sigv = torch.empty(n_vf * z.sig_bytes, dtype=torch.uint8).pin_memory()
+        torch.cuda.synchronize()
+        h_sigv.copy_(d_sig_vf)
+        h2d_list += [(d_seeds, h_seeds), (d_msg_sg, h_msgs), (d_msg_vf, h_msgv), (d_sig_vf, h_sigv)]
+        h_res_s = torch.empty(n_vf, dtype=torch.uint8).pin_memory()
+        h_res_parts.append(h_res_s)
+        d2h_list += [(torch.empty(n_kp * z.pk_bytes, dtype=torch.uint8).pin_memory(), d_pk),
+                     (torch.empty(n_sg * z.sig_bytes, dtype=torch.uint8).pin_memory(), d_sig_sg),
+                     (h_res_s, d_res)]
+    rng = np.random.default_rng(seed)
+    items = Q.items_array([entries[i] for i in rng.permutation(len(entries))])
+    q = Q.Queue(capacity=batch + batch // 8 + 64)
+    for s, ops in operands.items():
+        q.set_operands(s, ops)
+    tuned = AT.tune_queue(q, items)
+    q.capture()
+
+    def queue_op():
+        q.replay()
+
+    def plain():
+        for (m, kpool, kpch, n_kp, esk, epk, d_msg_sg, d_sig_sg, n_sg, d_msg_vf, d_sig_vf, d_res, n_vf,
+             ws) in plain_parts:
+            m.crypto_sign_keypair_from_seed(kpool, kpch, n_kp, st)
+            m.sign_many(esk, d_msg_sg, d_sig_sg, ws, n_sg, msg_stride=mlen, mlen=mlen, stream=st)
+            m.verify_many(epk, d_msg_vf, d_sig_vf, d_res, n_vf, msg_stride=mlen, mlen=mlen, stream=st)
+
+    def h2d():
+        for d, h in h2d_list:
+            d.copy_(h, non_blocking=True)
+
+    def d2h():
+        for h, d in d2h_list:
+            h.copy_(d, non_blocking=True)
+
+    all_res = [ops.vf_res for ops in operands.values()]
+    n_vf_total = sum(int(r.numel()) for r in all_res)
+    expected = np.zeros(n_vf_total, np.uint8)
+    res_dev = lambda: torch.cat(all_res)  # noqa: E731
+    class _HostRes:  # host copies of every set's verify results, concatenated like res_dev()
+        def numpy(self):
+            return torch.cat(h_res_parts).numpy()
+
+    h_res = _HostRes()
+    h2d_bytes = sum(int(h.numel()) for _, h in h2d_list)
+    d2h_bytes = sum(int(d.numel()) for _, d in d2h_list)
+    cfg = {"workload": "mixed MAYO_1/2/3/5 x {keypair, sign, verify} in one persistent queue launch",
+           "batch": batch, "msg_len": f"{mlen} B", "keys": "caller-seeded keypairs; one resident key per set "
+                                                          "for sign/verify",
+           "queue": {"ctas": q.ctas, "order": tuned["order"], "capacity": q.capacity,
+                     "autotune_trials": tuned.get("trials")},
+           "graph": "CUDA graph (queue reset + persistent kernel) replayed per step",
+           "l2": "flushed between steps (256 MiB write)"}
+    return ([("queue", queue_op)], h2d, d2h, h2d_bytes, d2h_bytes, batch, {"queue": work_macs},
+            {"queue": 0}, cfg, expected, res_dev, h_res, plain, 2)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -782,7 +923,7 @@ def run_reference_pool(args, dist: Dist, path: str):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))

@@ -157,7 +157,7 @@ __device__ __forceinline__ void st16(uint8_t *p, uint32_t a, uint32_t b, uint32_
 constexpr int AES_THREADS = 256;
 constexpr int AES_BLOCKS_PER_CTA = 2048;
 
-__global__ void __launch_bounds__(AES_THREADS) aes_ctr_kernel(uint8_t *pool, size_t pitch, size_t key_off,
+static __global__ void __launch_bounds__(AES_THREADS) aes_ctr_kernel(uint8_t *pool, size_t pitch, size_t key_off,
                                                                size_t out_off, uint32_t nblk_main) {
     extern __shared__ uint32_t aes_smem[];  // 256 * 32 words
     __shared__ uint32_t rk_s[44];
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(AES_THREADS) aes_ctr_kernel(uint8_t *pool, siz
 }
 
 // Blocks [nblk_main, ceil(nbytes/16)) for each instance (key read before any byte is written).
-__global__ void aes_ctr_tail_kernel(uint8_t *pool, size_t pitch, size_t key_off, size_t out_off,
+static __global__ void aes_ctr_tail_kernel(uint8_t *pool, size_t pitch, size_t key_off, size_t out_off,
                                     uint32_t nblk_main, uint32_t nbytes, uint32_t batch) {
     uint32_t inst = blockIdx.x * blockDim.x + threadIdx.x;
     if (inst >= batch) return;

@@ -23,7 +23,9 @@
 namespace mayo {
 
 // Packed bytes [p, p + n) (n <= 16) of an m-vector group as four LE words, touching only
-// aligned 32-bit words that contain at least one requested byte.
+// aligned 32-bit words that contain at least one requested byte.  RO selects the read-only
+// (non-coherent) load path, valid only for data no thread writes during the kernel.
+template <bool RO = true>
 __device__ __forceinline__ void load_group_words(const uint8_t *p, int n, uint32_t &w0, uint32_t &w1, uint32_t &w2,
                                                  uint32_t &w3) {
     const uintptr_t a = reinterpret_cast<uintptr_t>(p);
@@ -33,7 +35,7 @@ __device__ __forceinline__ void load_group_words(const uint8_t *p, int n, uint32
     const int nw = (int)(((a & 3) + n + 3) >> 2);
     uint32_t x[5];
 #pragma unroll
-    for (int i = 0; i < 5; i++) x[i] = i < nw ? __ldg(q + i) : 0u;
+    for (int i = 0; i < 5; i++) x[i] = i < nw ? (RO ? __ldg(q + i) : q[i]) : 0u;
     w0 = __funnelshift_r(x[0], x[1], sh);
     w1 = __funnelshift_r(x[1], x[2], sh);
     w2 = __funnelshift_r(x[2], x[3], sh);
@@ -57,12 +59,23 @@ __device__ __forceinline__ int group_bytes(int w) {
     return min(16, MENC - 16 * w);
 }
 
-template <int SET>
+template <int SET, bool RO = true>
 __device__ __forceinline__ G4 load_group(const uint8_t *entry, int w) {
     uint32_t w0, w1, w2, w3;
-    load_group_words(entry + 16 * w, group_bytes<Set<SET>::menc>(w), w0, w1, w2, w3);
+    load_group_words<RO>(entry + 16 * w, group_bytes<Set<SET>::menc>(w), w0, w1, w2, w3);
     return g4_from_packed(w0, w1, w2, w3);
 }
+
+// Rows functors may declare `static constexpr bool read_only = false;` when their entries are
+// written during the same kernel; the default is the read-only load path.
+template <class Rows, class = void>
+struct RowsReadOnly {
+    static constexpr bool value = true;
+};
+template <class Rows>
+struct RowsReadOnly<Rows, decltype((void)Rows::read_only)> {
+    static constexpr bool value = Rows::read_only;
+};
 
 // Write bit-plane group g (group w of an m-vector) as packed bytes to any address.
 template <int SET>
@@ -130,7 +143,7 @@ struct Engine {
             for (int idx = tid; idx < cnt * W; idx += nthreads) {
                 const int e = idx / W, ww = idx - e * W;
                 const uint8_t *src = rows.entry(r, e);
-                G4 g = src ? load_group<SET>(src, ww) : g4_zero();
+                G4 g = src ? load_group<SET, RowsReadOnly<Rows>::value>(src, ww) : g4_zero();
                 g4_st(dst + idx, g);
             }
         }

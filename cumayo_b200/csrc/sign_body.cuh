@@ -1,0 +1,583 @@
+// sign_body.cuh -- one MAYO signature on one CTA (reference src/sign.cu:10-477), shared by the
+// batched sign kernel and the persistent work-queue kernel.
+//
+//   U = V^T P1 V and y = sum z^l U_l + t        engine over P1 rows          (sign.cu:396-460)
+//   M_i = V_i L                                  engine over the columns of L (sign.cu:256-330)
+//   A = sum z^l M                                packed z-shifts, one thread per column (sign.cu:333-393)
+//   x = solve(A, y, r)                           constant-time Gauss-Jordan over bit-planes (sign.cu:10-145)
+// Every value derived from the secret key enters arithmetic only through masks, so no branch
+// or shared-memory address depends on it; only the attempt count is data dependent, as in MAYO.
+//
+// Why the elimination may differ from the reference's and still give identical bytes: when
+// rank A = m, the reference's pivot columns are the lexicographically first column basis of A
+// (a property of A alone), and x = r + z with z the unique vector supported on those columns
+// solving A z = y - A r.  Gauss-Jordan with any pivot-row choice finds the same columns and the
+// same z.  Rank < m is detected by both (the reference: last echelon row zero).
+#pragma once
+
+#include "engine.cuh"
+#include "launch_util.cuh"
+#include "ops.h"
+
+namespace mayo {
+
+// Workspace layout inside the row's scratch region (k*m*ceil(o/2) bytes, at least 2304).
+template <int SET>
+struct SignWs {
+    using S = Set<SET>;
+    static constexpr int dig = 0, salt = S::digest, t = S::digest + S::sk, vr = S::digest + S::sk + S::menc;
+    static constexpr int total = vr + S::vr;
+    static_assert(total <= S::scratch, "workspace fits the reference scratch region");
+};
+
+template <int SET, int NT_ = 0>
+struct SignCfg {
+    using S = Set<SET>;
+    static constexpr int J = S::k, W = S::W;
+    static constexpr int R = SET == 2 ? 16 : (SET == 1 ? 4 : 2);
+    static constexpr int NT = NT_ ? NT_ : (SET == 5 ? 160 : 128);
+    static constexpr int NCOL = S::ko + 1;  // columns of [A | y]
+    static constexpr int CPT = (NCOL + NT - 1) / NT;
+    static constexpr int NW = (S::menc + 3) / 4;
+    static_assert(J * W * R <= NT, "engine threads");
+    // shared memory (bytes); the bit-plane columns of A reuse the engine staging area
+    static constexpr size_t off_masks = 0;
+    static constexpr size_t off_bs = off_masks + (size_t)S::v * J * 16;
+    static constexpr size_t sz_bs = (size_t)R * S::n * W * 16;
+    static constexpr size_t sz_acol = (size_t)NCOL * W * 16;
+    static constexpr size_t off_x = off_bs + (sz_bs > sz_acol ? sz_bs : sz_acol);
+    static constexpr size_t off_upk = off_x + (size_t)J * J * W * 16;
+    static constexpr size_t off_mpk = off_upk + pad16((size_t)S::pairs * NW * 4);
+    static constexpr size_t off_piv = off_mpk + pad16((size_t)S::k * S::o * NW * 4);
+    static constexpr size_t off_rhs = off_piv + (size_t)2 * (W + 2) * 16;
+    static constexpr size_t off_y = off_rhs + (size_t)W * 16;
+    static constexpr size_t off_key = off_y + pad16(NW * 4);
+    static constexpr size_t off_t = off_key + pad16(S::digest + 2 * S::sk + 1);
+    static constexpr size_t off_vr = off_t + pad16(NW * 4);
+    static constexpr size_t off_xs = off_vr + pad16(S::vr);
+    static constexpr size_t off_flag = off_xs + pad16(S::ko);
+    static constexpr size_t total = off_flag + 16;
+};
+
+template <int SET>
+struct P1Rows {  // rows r < v of the upper-triangular P1 (sign.cu:402-418)
+    using S = Set<SET>;
+    const uint8_t *P1;
+    __device__ __forceinline__ int count(int r) const { return S::v - r; }
+    __device__ __forceinline__ const uint8_t *entry(int r, int e) const {
+        return P1 + (size_t)tri(r, r + e, S::v) * S::menc;
+    }
+    __device__ __forceinline__ int col(int r, int e) const { return r + e; }
+};
+
+template <int SET>
+struct LColRows {  // "row" b = column b of L: entries L[a][b], a < v (sign.cu:274-319)
+    using S = Set<SET>;
+    const uint8_t *L;
+    __device__ __forceinline__ int count(int) const { return S::v; }
+    __device__ __forceinline__ const uint8_t *entry(int b, int a) const {
+        return L + (size_t)(a * S::o + b) * S::menc;
+    }
+    __device__ __forceinline__ int col(int, int a) const { return a; }
+};
+
+__device__ __forceinline__ int pair_index_s(int i, int j, int k) { return i * k - (i * (i - 1)) / 2 + (j - i); }
+// Position of pair (a <= b) in the A-assembly order (sign.cu:333-392): i = 0..k-1, j = k-1..i.
+__device__ __forceinline__ int ell_of(int a, int b, int k) { return a * k - (a * (a - 1)) / 2 + (k - 1 - b); }
+
+// Packed word q (8 coordinates) of z^ell * u for a packed m-vector u (NW words in shared memory),
+// without the fold: coordinates >= m are dropped.
+template <int SET>
+__device__ __forceinline__ uint32_t zshift_word(const uint32_t *u, int q, int ell) {
+    using S = Set<SET>;
+    constexpr int NW = (S::menc + 3) / 4;
+    const int Q = ell >> 3, sh = (ell & 7) * 4;
+    const int qa = q - Q, qb = q - Q - 1;
+    const uint32_t a = (qa >= 0 && qa < NW) ? u[qa] : 0u;
+    const uint32_t b = (qb >= 0 && qb < NW) ? u[qb] : 0u;
+    uint32_t w = sh ? ((a << sh) | (b >> (32 - sh))) : a;
+    if (q == S::m / 8 && (S::m % 8)) w &= (1u << (4 * (S::m % 8))) - 1;
+    if (q >= (S::m + 7) / 8) w = 0;
+    return w;
+}
+// Packed word q of u >> (4 * shift) coordinates (shift > 0): coordinates shift.. move to 0..
+template <int SET>
+__device__ __forceinline__ uint32_t zdown_word(const uint32_t *u, int q, int shift) {
+    using S = Set<SET>;
+    constexpr int NW = (S::menc + 3) / 4;
+    const int Q = shift >> 3, sh = (shift & 7) * 4;
+    const int qa = q + Q, qb = q + Q + 1;
+    const uint32_t a = (qa < NW) ? u[qa] : 0u;
+    const uint32_t b = (qb < NW) ? u[qb] : 0u;
+    return sh ? ((a >> sh) | (b << (32 - sh))) : a;
+}
+
+// Shared-memory views of one signing CTA.
+#define MAYO_SIGN_VIEWS                                                                       \
+    using S = Set<SET>;                                                                       \
+    using C = SignCfg<SET, NT_>;                                                              \
+    constexpr int J = C::J, W = C::W, R = C::R, NT = C::NT, NW = C::NW, KO = S::ko, CPT = C::CPT; \
+    (void)J; (void)R; (void)KO; (void)CPT; (void)NW;
+
+// Plain path: digest, salt, t and V||r(ctr = 0) from the workspace written by sign_hash_kernel.
+template <int SET, int NT_>
+__device__ __forceinline__ void sign_load_ws(uint8_t *smem, int tid, const uint8_t *esk, const uint8_t *ws) {
+    MAYO_SIGN_VIEWS
+    uint4 *masks = reinterpret_cast<uint4 *>(smem + C::off_masks);
+    uint4 *bs = reinterpret_cast<uint4 *>(smem + C::off_bs);
+    uint4 *acol = reinterpret_cast<uint4 *>(smem + C::off_bs);  // [NCOL][W], after the engine phases
+    uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
+    uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
+    uint32_t *mpk = reinterpret_cast<uint32_t *>(smem + C::off_mpk);  // [k][o][NW]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W]
+    uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);     // [W]
+    uint32_t *ypk = reinterpret_cast<uint32_t *>(smem + C::off_y);
+    uint8_t *s_key = smem + C::off_key;  // digest || salt || seed_sk || ctr
+    uint8_t *s_t = smem + C::off_t;
+    uint8_t *s_vr = smem + C::off_vr;
+    uint8_t *s_x = smem + C::off_xs;
+    int *s_flag = reinterpret_cast<int *>(smem + C::off_flag);
+    (void)masks; (void)bs; (void)acol; (void)xacc; (void)upk; (void)mpk; (void)pivbuf; (void)rhsacc; (void)ypk; (void)s_key; (void)s_t; (void)s_vr; (void)s_x; (void)s_flag;
+    using WS = SignWs<SET>;
+    for (int i = tid; i < S::digest + S::sk; i += NT) s_key[i] = ws[WS::dig + i];
+    for (int i = tid; i < S::sk; i += NT) s_key[S::digest + S::sk + i] = esk[i];
+    for (int i = tid; i < NW * 4; i += NT) s_t[i] = i < S::menc ? ws[WS::t + i] : 0;
+    for (int i = tid; i < S::vr; i += NT) s_vr[i] = ws[WS::vr + i];
+    __syncthreads();
+}
+
+// Queue path: the CTA hashes itself (warp 0, warp-cooperative Keccak): digest = SHAKE256(M),
+// salt = SHAKE256(digest || 0^SK || seed_sk), t = SHAKE256(digest || salt), V || r for `ctr`
+// (sign.cu:225-252).  All threads must call it.
+template <int SET, int NT_>
+__device__ __forceinline__ void sign_hash_cta(uint8_t *smem, int tid, const uint8_t *esk, const uint8_t *msg,
+                                              uint32_t mlen, int ctr) {
+    MAYO_SIGN_VIEWS
+    uint4 *masks = reinterpret_cast<uint4 *>(smem + C::off_masks);
+    uint4 *bs = reinterpret_cast<uint4 *>(smem + C::off_bs);
+    uint4 *acol = reinterpret_cast<uint4 *>(smem + C::off_bs);  // [NCOL][W], after the engine phases
+    uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
+    uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
+    uint32_t *mpk = reinterpret_cast<uint32_t *>(smem + C::off_mpk);  // [k][o][NW]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W]
+    uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);     // [W]
+    uint32_t *ypk = reinterpret_cast<uint32_t *>(smem + C::off_y);
+    uint8_t *s_key = smem + C::off_key;  // digest || salt || seed_sk || ctr
+    uint8_t *s_t = smem + C::off_t;
+    uint8_t *s_vr = smem + C::off_vr;
+    uint8_t *s_x = smem + C::off_xs;
+    int *s_flag = reinterpret_cast<int *>(smem + C::off_flag);
+    (void)masks; (void)bs; (void)acol; (void)xacc; (void)upk; (void)mpk; (void)pivbuf; (void)rhsacc; (void)ypk; (void)s_key; (void)s_t; (void)s_vr; (void)s_x; (void)s_flag;
+    uint8_t *s_salt = s_x;  // s_x is free until the attempt writes x
+    if (tid < 32) {
+        const int lane = tid;
+        WarpKeccak wk;
+        wk.setup(lane);
+        warp_shake<136>(s_key, S::digest, msg, (int)mlen, wk, lane);
+        for (int i = lane; i < S::sk; i += 32) {
+            s_key[S::digest + i] = 0;
+            s_key[S::digest + S::sk + i] = esk[i];
+        }
+        if (lane == 0) s_key[S::digest + 2 * S::sk] = (uint8_t)ctr;
+        __syncwarp();
+        warp_shake<136>(s_salt, S::sk, s_key, S::digest + 2 * S::sk, wk, lane);
+        for (int i = lane; i < S::sk; i += 32) s_key[S::digest + i] = s_salt[i];
+        for (int i = lane; i < NW * 4; i += 32) s_t[i] = 0;
+        __syncwarp();
+        warp_shake<136>(s_t, S::menc, s_key, S::digest + S::sk, wk, lane);
+        warp_shake<136>(s_vr, S::vr, s_key, S::digest + 2 * S::sk + 1, wk, lane);
+    }
+    __syncthreads();
+}
+
+// V || r for attempt `ctr` from the digest, salt and seed already in shared memory.
+template <int SET, int NT_>
+__device__ __forceinline__ void sign_next_vr(uint8_t *smem, int tid, int ctr) {
+    MAYO_SIGN_VIEWS
+    uint4 *masks = reinterpret_cast<uint4 *>(smem + C::off_masks);
+    uint4 *bs = reinterpret_cast<uint4 *>(smem + C::off_bs);
+    uint4 *acol = reinterpret_cast<uint4 *>(smem + C::off_bs);  // [NCOL][W], after the engine phases
+    uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
+    uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
+    uint32_t *mpk = reinterpret_cast<uint32_t *>(smem + C::off_mpk);  // [k][o][NW]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W]
+    uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);     // [W]
+    uint32_t *ypk = reinterpret_cast<uint32_t *>(smem + C::off_y);
+    uint8_t *s_key = smem + C::off_key;  // digest || salt || seed_sk || ctr
+    uint8_t *s_t = smem + C::off_t;
+    uint8_t *s_vr = smem + C::off_vr;
+    uint8_t *s_x = smem + C::off_xs;
+    int *s_flag = reinterpret_cast<int *>(smem + C::off_flag);
+    (void)masks; (void)bs; (void)acol; (void)xacc; (void)upk; (void)mpk; (void)pivbuf; (void)rhsacc; (void)ypk; (void)s_key; (void)s_t; (void)s_vr; (void)s_x; (void)s_flag;
+    if (tid < 32) {
+        const int lane = tid;
+        WarpKeccak wk;
+        wk.setup(lane);
+        if (lane == 0) s_key[S::digest + 2 * S::sk] = (uint8_t)ctr;
+        __syncwarp();
+        warp_shake<136>(s_vr, S::vr, s_key, S::digest + 2 * S::sk + 1, wk, lane);
+    }
+    __syncthreads();
+}
+
+// One attempt on the V || r in shared memory: x on success, x = r on a singular system.
+// Returns whether the system had full rank (uniform over the CTA).  All threads must call it.
+template <int SET, int NT_>
+__device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8_t *esk) {
+    MAYO_SIGN_VIEWS
+    uint4 *masks = reinterpret_cast<uint4 *>(smem + C::off_masks);
+    uint4 *bs = reinterpret_cast<uint4 *>(smem + C::off_bs);
+    uint4 *acol = reinterpret_cast<uint4 *>(smem + C::off_bs);  // [NCOL][W], after the engine phases
+    uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
+    uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
+    uint32_t *mpk = reinterpret_cast<uint32_t *>(smem + C::off_mpk);  // [k][o][NW]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W]
+    uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);     // [W]
+    uint32_t *ypk = reinterpret_cast<uint32_t *>(smem + C::off_y);
+    uint8_t *s_key = smem + C::off_key;  // digest || salt || seed_sk || ctr
+    uint8_t *s_t = smem + C::off_t;
+    uint8_t *s_vr = smem + C::off_vr;
+    uint8_t *s_x = smem + C::off_xs;
+    int *s_flag = reinterpret_cast<int *>(smem + C::off_flag);
+    (void)masks; (void)bs; (void)acol; (void)xacc; (void)upk; (void)mpk; (void)pivbuf; (void)rhsacc; (void)ypk; (void)s_key; (void)s_t; (void)s_vr; (void)s_x; (void)s_flag;
+    const int lane = tid & 31;
+    (void)lane;
+    const uint8_t *P1 = esk + S::sk + S::o_bytes;
+    const uint8_t *L = P1 + S::p1;
+    Engine<SET, J, R> eng;
+    eng.setup(masks, bs, tid);
+    // ---- masks of V: masks[c][i] = V_i[c] ----
+    for (int idx = tid; idx < S::v * J; idx += NT) {
+        const int c = idx / J, i = idx - c * J;
+        const int q = i * S::m + c;
+        masks[idx] = scalar_masks((s_vr[q >> 1] >> ((q & 1) * 4)) & 0xF);
+    }
+    for (int i = tid; i < J * J * W * 4; i += NT) reinterpret_cast<uint32_t *>(xacc)[i] = 0;
+    __syncthreads();
+
+    // ---- U = V^T P1 V ----
+    {
+        const P1Rows<SET> rows{P1};
+        G4 X[J];
+#pragma unroll
+        for (int i = 0; i < J; i++) X[i] = g4_zero();
+#pragma unroll 1
+        for (int r0 = 0; r0 < S::v; r0 += R) {
+            eng.convert(rows, r0, S::v, tid, NT);
+            __syncthreads();
+            const int r = r0 + eng.rs;
+            if (eng.active && r < S::v) {
+                const G4 T = eng.row_product(rows, r);
+                const uint4 *mr = masks + (size_t)r * J;
+#pragma unroll
+                for (int i = 0; i < J; i++) g4_madd(X[i], T, mr[i]);
+            }
+            __syncthreads();
+        }
+        if (eng.active) {
+#pragma unroll
+            for (int i = 0; i < J; i++) g4_atomic_xor(xacc + ((size_t)i * J + eng.j) * W + eng.w, X[i]);
+        }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < S::pairs * W; idx += NT) {
+        const int pid = idx / W, ww = idx - pid * W;
+        int i = 0, rem = pid;
+        while (rem >= J - i) {
+            rem -= J - i;
+            i++;
+        }
+        const int j = i + rem;
+        G4 u = g4_ld(xacc + ((size_t)i * J + j) * W + ww);
+        if (i != j) u = g4_xor(u, g4_ld(xacc + ((size_t)j * J + i) * W + ww));
+        const uint4 pk = g4_to_packed(u);
+        const uint32_t wd[4] = {pk.x, pk.y, pk.z, pk.w};
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if (4 * ww + q < NW) upk[pid * NW + 4 * ww + q] = wd[q];
+    }
+    __syncthreads();
+
+    // ---- y = sum z^l U_l + t (warp 0) while the others compute M = V L ----
+    if (tid < 32) {
+        uint32_t y = 0;
+#pragma unroll 1
+        for (int i = S::k - 1; i >= 0; i--)
+#pragma unroll 1
+            for (int j = i; j < S::k; j++) {
+                y = times_z_lane<SET>(y, lane);
+                if (lane < NW) y ^= upk[pair_index_s(i, j, S::k) * NW + lane];
+            }
+        if (lane < NW) ypk[lane] = y ^ reinterpret_cast<const uint32_t *>(s_t)[lane];
+    }
+    {
+        const LColRows<SET> rows{L};
+#pragma unroll 1
+        for (int b0 = 0; b0 < S::o; b0 += R) {
+            eng.convert(rows, b0, S::o, tid, NT);
+            __syncthreads();
+            const int b = b0 + eng.rs;
+            if (eng.active && b < S::o) {
+                const G4 T = eng.row_product(rows, b);  // M_j[b], j = eng.j
+                const uint4 pk = g4_to_packed(T);
+                const uint32_t wd[4] = {pk.x, pk.y, pk.z, pk.w};
+                uint32_t *dst = mpk + ((size_t)eng.j * S::o + b) * NW;
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    if (4 * eng.w + q < NW) dst[4 * eng.w + q] = wd[q];
+            }
+            __syncthreads();
+        }
+    }
+
+    // ---- A columns (i, b) = sum_j z^{l(i,j)} M_j[b] with one fold by f(z); RHS column = y ----
+    for (int c = tid; c < C::NCOL; c += NT) {
+        uint32_t acc[NW];
+#pragma unroll
+        for (int q = 0; q < NW; q++) acc[q] = 0;
+        if (c < KO) {
+            const int i = c / S::o, b = c - i * S::o;
+#pragma unroll 1
+            for (int j = 0; j < S::k; j++) {
+                const int ell = i <= j ? ell_of(i, j, S::k) : ell_of(j, i, S::k);
+                const uint32_t *u = mpk + ((size_t)j * S::o + b) * NW;
+#pragma unroll
+                for (int q = 0; q < NW; q++) acc[q] ^= zshift_word<SET>(u, q, ell);
+                if (ell > 0) {
+                    // overflow coordinates m-ell..m-1 -> 0..ell-1, times z^n * c_n for n = 0..3
+                    uint32_t ov[NW];
+#pragma unroll
+                    for (int q = 0; q < NW; q++) ov[q] = zdown_word<SET>(u, q, S::m - ell);
+                    // mask coordinates >= ell
+#pragma unroll
+                    for (int q = 0; q < NW; q++) {
+                        const int lo = 8 * q;
+                        if (lo >= ell) ov[q] = 0;
+                        else if (lo + 8 > ell) ov[q] &= (1u << (4 * (ell - lo))) - 1;
+                    }
+#pragma unroll
+                    for (int n = 0; n < 4; n++) {
+                        if (S::cf(n) == 0) continue;
+                        uint32_t prev = 0;
+#pragma unroll
+                        for (int q = 0; q < NW; q++) {
+                            const uint32_t mc = nib8_mul_const(ov[q], S::cf(n));
+                            acc[q] ^= n ? ((mc << (4 * n)) | (prev >> (32 - 4 * n))) : mc;
+                            prev = mc;
+                        }
+                    }
+                }
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < NW; q++) acc[q] = ypk[q];
+        }
+        // packed -> bit-planes
+#pragma unroll
+        for (int w = 0; w < W; w++) {
+            const uint32_t a0 = 4 * w + 0 < NW ? acc[4 * w + 0] : 0u;
+            const uint32_t a1 = 4 * w + 1 < NW ? acc[4 * w + 1] : 0u;
+            const uint32_t a2 = 4 * w + 2 < NW ? acc[4 * w + 2] : 0u;
+            const uint32_t a3 = 4 * w + 3 < NW ? acc[4 * w + 3] : 0u;
+            g4_st(acol + (size_t)c * W + w, g4_from_packed(a0, a1, a2, a3));
+        }
+    }
+    for (int i = tid; i < W * 4; i += NT) reinterpret_cast<uint32_t *>(rhsacc)[i] = 0;
+    __syncthreads();
+
+    // ---- Gauss-Jordan in constant time.  Thread owns columns c = tid + NT*q. ----
+    G4 col[CPT][W];
+    uint32_t rr[CPT];
+#pragma unroll
+    for (int q = 0; q < CPT; q++) {
+        const int c = tid + NT * q;
+#pragma unroll
+        for (int w = 0; w < W; w++) col[q][w] = c < C::NCOL ? g4_ld(acol + (size_t)c * W + w) : g4_zero();
+        const int rn = S::k * S::m;  // r starts after the k V-vectors (sign.cu:250)
+        rr[q] = c < KO ? (s_vr[(rn + c) >> 1] >> (((rn + c) & 1) * 4)) & 0xF : 0u;
+    }
+    // y <- y - A r  (sample_solution, sign.cu:36-45)
+#pragma unroll
+    for (int q = 0; q < CPT; q++) {
+        const int c = tid + NT * q;
+        if (c < KO) {
+            const uint4 mk = scalar_masks(rr[q]);
+#pragma unroll
+            for (int w = 0; w < W; w++) {
+                G4 pr = g4_zero();
+                g4_madd(pr, col[q][w], mk);
+                g4_atomic_xor(rhsacc + w, pr);
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < CPT; q++)
+        if (tid + NT * q == KO)
+#pragma unroll
+            for (int w = 0; w < W; w++) col[q][w] = g4_xor(col[q][w], g4_ld(rhsacc + w));
+
+    uint32_t pivoted[W];
+    uint32_t my_oh[CPT][W], my_has[CPT];
+#pragma unroll
+    for (int w = 0; w < W; w++) pivoted[w] = 0;
+#pragma unroll
+    for (int q = 0; q < CPT; q++) {
+        my_has[q] = 0;
+#pragma unroll
+        for (int w = 0; w < W; w++) my_oh[q][w] = 0;
+    }
+#pragma unroll 1
+    for (int pc = 0; pc < KO; pc++) {
+        // The owner of column pc computes the pivot (lowest unpivoted row with a nonzero
+        // entry), its inverse and F' = inv * (a + e_p), and publishes F' and the row one-hot.
+        uint4 *buf = pivbuf + (pc & 1) * (W + 2);
+        uint32_t *ohw = reinterpret_cast<uint32_t *>(buf + W);  // oh[0..W), found at [7]
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+            if (tid + NT * q != pc) continue;
+            uint32_t oh[W], found = 0;
+#pragma unroll
+            for (int w = 0; w < W; w++) {
+                const G4 &a = col[q][w];
+                const uint32_t nz = (a.p0 | a.p1 | a.p2 | a.p3) & ~pivoted[w];
+                const uint32_t low = nz & (0u - nz);
+                oh[w] = low & ~found;
+                found |= 0u - (uint32_t)(nz != 0u);
+            }
+            uint32_t o0 = 0, o1 = 0, o2 = 0, o3 = 0;
+#pragma unroll
+            for (int w = 0; w < W; w++) {
+                o0 |= col[q][w].p0 & oh[w];
+                o1 |= col[q][w].p1 & oh[w];
+                o2 |= col[q][w].p2 & oh[w];
+                o3 |= col[q][w].p3 & oh[w];
+            }
+            const uint32_t piv = (uint32_t)(o0 != 0) | ((uint32_t)(o1 != 0) << 1) |
+                                 ((uint32_t)(o2 != 0) << 2) | ((uint32_t)(o3 != 0) << 3);
+            const uint4 inv_m = scalar_masks(gf16_inv_ct(piv) & found);
+#pragma unroll
+            for (int w = 0; w < W; w++) {
+                G4 ap = col[q][w];
+                ap.p0 ^= oh[w];
+                G4 F = g4_zero();
+                g4_madd(F, ap, inv_m);
+                g4_st(buf + w, F);
+                ohw[w] = oh[w];
+                my_oh[q][w] = oh[w];
+            }
+            ohw[7] = found;
+            my_has[q] = found;
+        }
+        __syncthreads();
+        // every column: col ^= col[p] * F'  (eliminates row p elsewhere, normalises row p)
+        G4 F[W];
+        uint32_t oh[W];
+#pragma unroll
+        for (int w = 0; w < W; w++) {
+            F[w] = g4_ld(buf + w);
+            oh[w] = ohw[w];
+        }
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+            uint32_t e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+#pragma unroll
+            for (int w = 0; w < W; w++) {
+                e0 |= col[q][w].p0 & oh[w];
+                e1 |= col[q][w].p1 & oh[w];
+                e2 |= col[q][w].p2 & oh[w];
+                e3 |= col[q][w].p3 & oh[w];
+            }
+            const uint32_t ev = (uint32_t)(e0 != 0) | ((uint32_t)(e1 != 0) << 1) | ((uint32_t)(e2 != 0) << 2) |
+                                ((uint32_t)(e3 != 0) << 3);
+            const uint4 em = scalar_masks(ev);
+#pragma unroll
+            for (int w = 0; w < W; w++) g4_madd(col[q][w], F[w], em);
+        }
+#pragma unroll
+        for (int w = 0; w < W; w++) pivoted[w] |= oh[w];
+    }
+    // rank test (sign.cu:107-115 rejects when the last echelon row is zero, i.e. rank < m)
+    int rank = 0;
+#pragma unroll
+    for (int w = 0; w < W; w++) rank += __popc(pivoted[w]);
+    const bool ok = rank == S::m;
+    // publish the reduced RHS; x = r + z (z_c = rhs[p(c)] on pivot columns)
+#pragma unroll
+    for (int q = 0; q < CPT; q++)
+        if (tid + NT * q == KO)
+#pragma unroll
+            for (int w = 0; w < W; w++) g4_st(rhsacc + w, col[q][w]);  // not a buffer still being read
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < CPT; q++) {
+        const int c = tid + NT * q;
+        if (c < KO) {
+            uint32_t z0 = 0, z1 = 0, z2 = 0, z3 = 0;
+#pragma unroll
+            for (int w = 0; w < W; w++) {
+                const G4 h = g4_ld(rhsacc + w);
+                z0 |= h.p0 & my_oh[q][w];
+                z1 |= h.p1 & my_oh[q][w];
+                z2 |= h.p2 & my_oh[q][w];
+                z3 |= h.p3 & my_oh[q][w];
+            }
+            const uint32_t z = ((uint32_t)(z0 != 0) | ((uint32_t)(z1 != 0) << 1) | ((uint32_t)(z2 != 0) << 2) |
+                                ((uint32_t)(z3 != 0) << 3)) & my_has[q];
+            // a rejected attempt leaves x = r (sign.cu:31-33, 115)
+            s_x[c] = (uint8_t)(rr[q] ^ (ok ? z : 0u));
+        }
+    }
+    if (tid == 0) s_flag[0] = ok ? 1 : 0;
+    __syncthreads();
+    return s_flag[0] != 0;
+}
+
+// s = V + O x, then salt (sign.cu:147-191, 474-477).
+template <int SET, int NT_>
+__device__ __forceinline__ void sign_write(uint8_t *smem, int tid, const uint8_t *esk, uint8_t *sig) {
+    MAYO_SIGN_VIEWS
+    uint4 *masks = reinterpret_cast<uint4 *>(smem + C::off_masks);
+    uint4 *bs = reinterpret_cast<uint4 *>(smem + C::off_bs);
+    uint4 *acol = reinterpret_cast<uint4 *>(smem + C::off_bs);  // [NCOL][W], after the engine phases
+    uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
+    uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
+    uint32_t *mpk = reinterpret_cast<uint32_t *>(smem + C::off_mpk);  // [k][o][NW]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W]
+    uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);     // [W]
+    uint32_t *ypk = reinterpret_cast<uint32_t *>(smem + C::off_y);
+    uint8_t *s_key = smem + C::off_key;  // digest || salt || seed_sk || ctr
+    uint8_t *s_t = smem + C::off_t;
+    uint8_t *s_vr = smem + C::off_vr;
+    uint8_t *s_x = smem + C::off_xs;
+    int *s_flag = reinterpret_cast<int *>(smem + C::off_flag);
+    (void)masks; (void)bs; (void)acol; (void)xacc; (void)upk; (void)mpk; (void)pivbuf; (void)rhsacc; (void)ypk; (void)s_key; (void)s_t; (void)s_vr; (void)s_x; (void)s_flag;
+    const uint8_t *O_g = esk + S::sk;
+    uint8_t *sigp = sig;
+    for (int bidx = tid; bidx < S::k * S::n / 2; bidx += NT) {
+        uint32_t nb[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int e = 2 * bidx + h, i = e / S::n, t = e - i * S::n;
+            uint32_t val;
+            if (t < S::m) {
+                uint32_t acc = 0;
+#pragma unroll
+                for (int q = 0; q < S::o; q++) {
+                    const int oi = t * S::o + q;
+                    const uint32_t ov = (O_g[oi >> 1] >> ((oi & 1) * 4)) & 0xF;
+                    acc ^= gf16_mul_ct(ov, s_x[i * S::o + q]);
+                }
+                const int vi = i * S::m + t;
+                val = ((s_vr[vi >> 1] >> ((vi & 1) * 4)) & 0xF) ^ acc;
+            } else {
+                val = s_x[i * S::o + (t - S::m)];
+            }
+            nb[h] = val;
+        }
+        sigp[bidx] = (uint8_t)(nb[0] | (nb[1] << 4));
+    }
+    for (int i = tid; i < S::sk; i += NT) sigp[S::k * S::n / 2 + i] = s_key[S::digest + i];
+}
+
+}  // namespace mayo

@@ -147,6 +147,55 @@ MAYO_B200_API int mayo_b200_verify_many(int set, const uint8_t *epk, size_t epk_
                                         size_t mlen, const uint8_t *sig, size_t sig_stride, uint8_t *result,
                                         size_t batch, void *stream);
 
+/* ---- Extension (no counterpart in the reference): persistent work queue ----
+ * One launch of `ctas` resident CTAs drains a device queue of keypair / sign / verify items of
+ * all four parameter sets.  A sign attempt with a singular system is re-enqueued with the next
+ * attempt counter instead of being retried in place.  Every wait inside the kernel is bounded;
+ * a queue that overflows or a wait that runs out ends the launch with an error code in the
+ * queue's control words instead of hanging.  Results are byte-identical to the batched calls.
+ *
+ * Operands per parameter set (device pointers; an op's pointers may be NULL if no item uses it):
+ *   keypair  instance i: seed = kp_seed + i*sk_bytes  -> pk at kp_pk + i*pk_bytes
+ *   sign     instance i: key = sg_esk + (i % sg_nkeys)*esk_bytes, message sg_msg + i*sg_mlen
+ *            (sg_mlen bytes) -> signature at sg_sig + i*sig_bytes
+ *   verify   instance i: key = vf_epk + (i % vf_nkeys)*epk_bytes, message vf_msg + i*vf_mlen,
+ *            signature vf_sig + i*sig_bytes -> result byte vf_res[i] (0 accept, 1 reject)
+ * Queue memory (mayo_b200_queue_mem_bytes bytes, device, caller-allocated): control words at
+ * offset 0 (uint32: [0] tickets taken, [1] items published, [2] items finished, [3] error,
+ * [4] re-enqueued signs), then the slots, then per-CTA scratch. */
+enum { MAYO_B200_OP_KEYPAIR = 0, MAYO_B200_OP_SIGN = 1, MAYO_B200_OP_VERIFY = 2 };
+enum { MAYO_B200_QUEUE_OK = 0, MAYO_B200_QUEUE_ERR_FULL = 1, MAYO_B200_QUEUE_ERR_TIMEOUT = 2 };
+typedef struct mayo_b200_queue_ops {
+    const uint8_t *kp_seed;
+    uint8_t *kp_pk;
+    const uint8_t *sg_esk;
+    uint32_t sg_nkeys;
+    const uint8_t *sg_msg;
+    uint32_t sg_mlen;
+    uint8_t *sg_sig;
+    const uint8_t *vf_epk;
+    uint32_t vf_nkeys;
+    const uint8_t *vf_msg;
+    uint32_t vf_mlen;
+    const uint8_t *vf_sig;
+    uint8_t *vf_res;
+} mayo_b200_queue_ops;
+/* Work item: op (MAYO_B200_OP_*), parameter set (1, 2, 3, 5), instance index < 2^20. */
+static inline uint32_t mayo_b200_queue_item(int op, int set, uint32_t instance) {
+    const uint32_t si = set == 1 ? 0u : set == 2 ? 1u : set == 3 ? 2u : 3u;
+    return ((uint32_t)op << 30) | (si << 28) | (instance & 0xFFFFFu);
+}
+/* Device bytes of queue memory for `capacity` slots and `ctas` resident CTAs. */
+MAYO_B200_API size_t mayo_b200_queue_mem_bytes(uint32_t capacity, uint32_t ctas);
+/* Resident CTAs per SM the queue kernel can hold on the current device (0 on error). */
+MAYO_B200_API int mayo_b200_queue_ctas_per_sm(void);
+/* Reset the queue to items[0..n) (device array) and run it to completion on `stream`.
+ * capacity >= n; room beyond n holds re-enqueued signs (n + n/8 + 64 is ample).  Asynchronous;
+ * graph-capturable (no allocation, no host synchronisation).  spin_limit 0 = default. */
+MAYO_B200_API int mayo_b200_queue_run(const mayo_b200_queue_ops ops[4], const uint32_t *items, uint32_t n,
+                                      void *queue_mem, uint32_t capacity, uint32_t ctas, uint32_t spin_limit,
+                                      void *stream);
+
 /* ---- Sign without caller workspace.  No counterpart in the reference API. ----
  * For callers that cannot allocate device memory (a service whose device-memory budget is
  * fixed at start-up, or a host program that owns the allocator and forbids a plug-in library
