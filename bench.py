@@ -587,15 +587,16 @@ def setup_mixed_queue(args, dist, batch, seed, st):
     h_res = _HostRes()
     h2d_bytes = sum(int(h.numel()) for _, h in h2d_list)
     d2h_bytes = sum(int(d.numel()) for _, d in d2h_list)
-    cfg = {"workload": "mixed MAYO_1/2/3/5 x {keypair, sign, verify} in one persistent queue launch",
+    cfg = {"workload": "mixed MAYO_1/2/3/5 x {keypair, sign, verify} in one persistent work queue "
+                       "(device partition by (set, op), one persistent kernel each on forked streams)",
            "batch": batch, "msg_len": f"{mlen} B", "keys": "caller-seeded keypairs; one resident key per set "
                                                           "for sign/verify",
-           "queue": {"ctas": q.ctas, "order": tuned["order"], "capacity": q.capacity,
-                     "autotune_trials": tuned.get("trials")},
-           "graph": "CUDA graph (queue reset + persistent kernel) replayed per step",
+           "queue": {"sms": q.shape.sms, "ctas_per_sm": tuned["ctas_per_sm"], "launch_order": tuned["launch_order"],
+                     "capacity": q.capacity, "autotune_trials": tuned.get("trials")},
+           "graph": "CUDA graph (queue reset, partition, 12 persistent (set, op) kernels) replayed per step",
            "l2": "flushed between steps (256 MiB write)"}
     return ([("queue", queue_op)], h2d, d2h, h2d_bytes, d2h_bytes, batch, {"queue": work_macs},
-            {"queue": 0}, cfg, expected, res_dev, h_res, plain, 2)
+            {"queue": 0}, cfg, expected, res_dev, h_res, plain, 14)
 
 
 # ---------------------------------------------------------------------------------------------

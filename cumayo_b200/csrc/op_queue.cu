@@ -1,15 +1,26 @@
-// op_queue.cu -- persistent work-queue kernel: keypair / sign / verify instances of all four
-// parameter sets pulled by resident CTAs from one device queue.
+// op_queue.cu -- persistent work queue: keypair / sign / verify items of all four parameter sets.
 //
 // A work item is a 32-bit word: op (2 bits), parameter-set index (2 bits: MAYO_1, 2, 3, 5),
-// sign attempt counter (8 bits) and instance index (20 bits).  Each CTA (160 threads) takes the
-// next item with an atomic ticket, runs it with the same device functions as the batched
-// kernels, and takes the next.  A sign attempt whose linear system is singular is not retried
-// in place: the CTA pushes (sign, ctr + 1) to the tail of the queue and moves on, so one rare
-// rejection never holds a CTA (or a whole launch) back.  The queue is drained when every
-// published item is finished (done == tail; `done` is read before `tail`, so a push from an
-// unfinished item can never be missed).  Waits are bounded: a ticket that stays unpublished past
-// `spin_limit` sleeps sets an error code and ends the CTA instead of hanging.
+// sign attempt counter (8 bits) and instance index (20 bits).  A run
+//   1. fills every bucket's slots with "empty" and zeroes the control words,
+//   2. partitions the caller's mixed item array into 12 buckets, one per (set, op), keeping the
+//      order within a bucket,
+//   3. forks streams and launches one persistent kernel per bucket whose operands are set.
+// Each (set, op) has its own kernel because their CTAs need 35-81 KB of shared memory and 56-128
+// registers per thread: one kernel shaped for the largest would run MAYO_1 at two CTAs per SM
+// instead of five, and MAYO_5's keypair and verify at two instead of three.  Each kernel has the
+// shape of the batched kernel for its (set, op).  On forked streams the kernels share the SMs,
+// and the CTAs of a kernel launched later take the SMs of one whose bucket has drained, so one
+// bucket's tail overlaps another's work.
+//
+// Inside a kernel each CTA takes the next item with an atomic ticket, runs it with the same
+// device functions as the batched kernels, and takes the next.  A sign attempt whose linear
+// system is singular is not retried in place: the CTA pushes (sign, ctr + 1) to the tail of its
+// bucket and moves on, so one rare rejection never holds a CTA back.  A bucket is drained when
+// every published item is finished (done == tail; `done` is read before `tail`, so a push from an
+// unfinished item can never be missed).  A CTA only ever waits for items held by CTAs of its own
+// kernel that are already running, so the kernels need not be co-resident.  Waits are bounded: a
+// ticket that stays unpublished past `spin_limit` sleeps sets an error code and ends the CTA.
 #include <cuda_runtime.h>
 
 #include "../../include/mayo_b200.h"
@@ -21,34 +32,55 @@
 
 namespace mayo {
 
-constexpr int Q_NT = 160;  // threads per queue CTA
-constexpr int Q_NCV = 128; // verify compute threads (+ one hashing warp)
 constexpr uint32_t Q_EMPTY = 0xFFFFFFFFu;
 constexpr uint32_t Q_STOP = 0xFFFFFFFEu;
+constexpr int Q_BUCKETS = 12;             // (set index) * 3 + op
+constexpr int Q_CTRL_WORDS = 16;          // control words per bucket; block 12 counts invalid ops
+constexpr size_t Q_SM_SMEM = 228 * 1024;  // shared memory per SM (sm_100)
+constexpr size_t Q_CTA_RESERVED = 1024;   // shared memory the runtime reserves per CTA
 
-__host__ __device__ constexpr int set_of_index(int si) { return si == 0 ? 1 : si == 1 ? 2 : si == 2 ? 3 : 5; }
+template <int SET, int OP>
+struct QueueCfg;
 
 template <int SET>
-struct QueueLayout {
-    using KC = KeyCfg<SET, Q_NT>;
+struct QueueCfg<SET, MAYO_B200_OP_KEYPAIR> {
+    using S = Set<SET>;
+    using KC = KeyCfg<SET>;
+    static constexpr int NT = KC::NT;
     static constexpr size_t aes_end = 256 * 32 * 4 + 44 * 4;  // replicated T0 + round keys
     static_assert(KC::off_o >= aes_end, "O must not overlap the AES tables");
-    static constexpr size_t kp_seedpk = KC::off_o + pad16(Set<SET>::o_bytes);
-    static constexpr size_t kp_total = kp_seedpk + 16;
-    static constexpr size_t total_raw = kp_total > SignCfg<SET, Q_NT>::total
-                                            ? (kp_total > VerifyCfg<SET, Q_NCV>::total ? kp_total
-                                                                                       : VerifyCfg<SET, Q_NCV>::total)
-                                            : (SignCfg<SET, Q_NT>::total > VerifyCfg<SET, Q_NCV>::total
-                                                   ? SignCfg<SET, Q_NT>::total
-                                                   : VerifyCfg<SET, Q_NCV>::total);
+    static constexpr size_t seedpk = KC::off_o + pad16(S::o_bytes);
+    static constexpr size_t smem = seedpk + 16;
+    static constexpr size_t scratch = pad16((size_t)S::p + 16);  // P1 || P2 of one keypair
 };
-static_assert(VerifyCfg<1, Q_NCV>::NT == Q_NT && VerifyCfg<5, Q_NCV>::NT == Q_NT, "verify CTA shape");
+
+template <int SET>
+struct QueueCfg<SET, MAYO_B200_OP_SIGN> {
+    static constexpr int NT = SignCfg<SET>::NT;
+    static constexpr size_t smem = SignCfg<SET>::total;
+    static constexpr size_t scratch = 0;
+};
+
+template <int SET>
+struct QueueCfg<SET, MAYO_B200_OP_VERIFY> {
+    static constexpr int NT = VerifyCfg<SET>::NT;
+    static constexpr size_t smem = VerifyCfg<SET>::total;
+    static constexpr size_t scratch = 0;
+};
+
+// CTAs of a bucket's kernel that fit in one SM's shared memory: the register budget per thread
+// is set so that registers do not lower the residency further.
+template <int SET, int OP>
+struct QueueFit {
+    static constexpr int fit = (int)(Q_SM_SMEM / (QueueCfg<SET, OP>::smem + Q_CTA_RESERVED));
+    static constexpr int MINB = fit > 8 ? 8 : (fit < 1 ? 1 : fit);
+};
 
 using QueueOps = mayo_b200_queue_ops;
 
 struct QueueArgs {
-    QueueOps ops[4];
-    uint32_t *items;
+    QueueOps ops;
+    uint32_t *slots;
     uint32_t capacity;
     uint32_t *ctrl;  // [0] head ticket, [1] tail, [2] done, [3] error, [4] pushes
     uint8_t *scratch;
@@ -58,11 +90,13 @@ struct QueueArgs {
 
 __device__ __forceinline__ uint32_t ld_volatile(const uint32_t *p) { return *reinterpret_cast<const volatile uint32_t *>(p); }
 
+__device__ __forceinline__ void queue_error(uint32_t *ctrl, uint32_t code) { atomicCAS(&ctrl[3], 0u, code); }
+
 __device__ uint32_t queue_pop(const QueueArgs &q) {
     const uint32_t idx = atomicAdd(&q.ctrl[0], 1u);
     for (uint32_t it = 0;; it++) {
         if (idx < q.capacity) {
-            const uint32_t v = ld_volatile(&q.items[idx]);
+            const uint32_t v = ld_volatile(&q.slots[idx]);
             if (v != Q_EMPTY) {
                 __threadfence();
                 return v;
@@ -75,7 +109,7 @@ __device__ uint32_t queue_pop(const QueueArgs &q) {
         // A ticket past the last slot can only end with the drain; a ticket inside the queue
         // waits for its item to be published.  Both waits are bounded.
         if (it >= q.spin_limit) {
-            atomicCAS(&q.ctrl[3], 0u, (uint32_t)MAYO_B200_QUEUE_ERR_TIMEOUT);
+            queue_error(q.ctrl, MAYO_B200_QUEUE_ERR_TIMEOUT);
             return Q_STOP;
         }
         __nanosleep(200);
@@ -85,26 +119,62 @@ __device__ uint32_t queue_pop(const QueueArgs &q) {
 __device__ void queue_push(const QueueArgs &q, uint32_t item) {
     const uint32_t slot = atomicAdd(&q.ctrl[1], 1u);
     if (slot >= q.capacity) {
-        atomicCAS(&q.ctrl[3], 0u, (uint32_t)MAYO_B200_QUEUE_ERR_FULL);
+        queue_error(q.ctrl, MAYO_B200_QUEUE_ERR_FULL);
         // the slot never becomes visible; count the item as finished so the queue still drains
         atomicAdd(&q.ctrl[2], 1u);
         return;
     }
     atomicAdd(&q.ctrl[4], 1u);
     __threadfence();
-    *reinterpret_cast<volatile uint32_t *>(&q.items[slot]) = item;
+    *reinterpret_cast<volatile uint32_t *>(&q.slots[slot]) = item;
+}
+
+// Operands of one instance, checked against the counts and key tables the caller declared.
+struct ItemRefs {
+    const uint8_t *key;
+    const uint8_t *msg;
+    uint32_t mlen;
+    bool ok;
+};
+
+template <int SET, int OP>
+__device__ ItemRefs queue_refs(const QueueOps &o, uint32_t inst) {
+    using S = Set<SET>;
+    ItemRefs r{nullptr, nullptr, 0, false};
+    if (OP == MAYO_B200_OP_KEYPAIR) {
+        r.ok = inst < o.kp_count && o.kp_seed && o.kp_pk;
+        return r;
+    }
+    constexpr bool sg = OP == MAYO_B200_OP_SIGN;
+    const uint8_t *keys = sg ? o.sg_esk : o.vf_epk;
+    const uint32_t nkeys = sg ? o.sg_nkeys : o.vf_nkeys, count = sg ? o.sg_count : o.vf_count;
+    const uint32_t *kidx = sg ? o.sg_key : o.vf_key;
+    const uint8_t *msgs = sg ? o.sg_msg : o.vf_msg;
+    const uint64_t *moff = sg ? o.sg_msg_off : o.vf_msg_off;
+    const uint32_t *mlen = sg ? o.sg_msg_len : o.vf_msg_len;
+    const uint32_t stride = sg ? o.sg_mlen : o.vf_mlen;
+    const bool outs = sg ? o.sg_sig != nullptr : (o.vf_sig != nullptr && o.vf_res != nullptr);
+    if (inst >= count || !keys || nkeys == 0 || !outs) return r;
+    const uint32_t k = kidx ? kidx[inst] : inst % nkeys;
+    if (k >= nkeys) return r;
+    r.key = keys + (size_t)k * (sg ? S::esk : S::epk);
+    r.mlen = mlen ? mlen[inst] : stride;
+    r.msg = msgs ? msgs + (moff ? moff[inst] : (uint64_t)inst * stride) : nullptr;
+    r.ok = r.msg != nullptr || r.mlen == 0;
+    if (!r.msg) r.msg = keys;  // zero-length message: any readable address
+    return r;
 }
 
 // ---- keypair from a caller seed on one CTA: hash (warp 0), AES-CTR (all), P3 (engine) ----
 template <int SET>
 __device__ void queue_keypair(uint8_t *smem, int tid, const QueueOps &ops, uint32_t inst, uint8_t *scratch) {
     using S = Set<SET>;
-    using QL = QueueLayout<SET>;
-    using KC = KeyCfg<SET, Q_NT>;
+    using QC = QueueCfg<SET, MAYO_B200_OP_KEYPAIR>;
+    constexpr int NT = QC::NT;
     const uint8_t *seed = ops.kp_seed + (size_t)inst * S::sk;
     uint8_t *pk = ops.kp_pk + (size_t)inst * S::pk;
-    uint8_t *s_O = smem + KC::off_o;
-    uint8_t *s_seedpk = smem + QL::kp_seedpk;
+    uint8_t *s_O = smem + QC::KC::off_o;
+    uint8_t *s_seedpk = smem + QC::seedpk;
     if (tid < 32) {
         // seed_pk || O = SHAKE256(seed_sk) (src/keypair.cu:47), squeezed into the AES area, which is
         // free until the tables are built below
@@ -119,7 +189,7 @@ __device__ void queue_keypair(uint8_t *smem, int tid, const QueueOps &ops, uint3
     // AES-CTR of P1 || P2 into this CTA's scratch (src/keypair.cu:52)
     uint32_t *T = reinterpret_cast<uint32_t *>(smem);
     uint32_t *rk_s = T + 256 * 32;
-    for (int i = tid; i < 256 * 32; i += Q_NT) T[i] = c_aes.te0[i >> 5];
+    for (int i = tid; i < 256 * 32; i += NT) T[i] = c_aes.te0[i >> 5];
     if (tid == 0) aes128_key_schedule(s_seedpk, rk_s);
     __syncthreads();
     {
@@ -128,66 +198,54 @@ __device__ void queue_keypair(uint8_t *smem, int tid, const QueueOps &ops, uint3
         for (int i = 0; i < 44; i++) rk[i] = rk_s[i];
         const uint32_t *Tl = T + (tid & 31);
         const uint32_t nblk = (S::p + 15) / 16;  // the scratch has room for the whole last block
-        for (uint32_t blk = tid; blk < nblk; blk += Q_NT) {
+        for (uint32_t blk = tid; blk < nblk; blk += NT) {
             const AesOut o = aes128_ctr_block(Tl, rk, blk);
             st16(scratch + (size_t)blk * 16, bswap32(o.w0), bswap32(o.w1), bswap32(o.w2), bswap32(o.w3));
         }
     }
     __syncthreads();  // scratch writes visible to the whole CTA; AES tables no longer needed
-    for (int i = tid; i < 16; i += Q_NT) pk[i] = s_seedpk[i];
-    p3_instance<SET, Q_NT, false>(smem, tid, scratch, scratch + S::p1, pk + 16);
+    for (int i = tid; i < 16; i += NT) pk[i] = s_seedpk[i];
+    p3_instance<SET, NT, false>(smem, tid, scratch, scratch + S::p1, pk + 16);
 }
 
 template <int SET>
-__device__ void queue_sign(uint8_t *smem, int tid, const QueueArgs &q, const QueueOps &ops, uint32_t inst, int ctr,
+__device__ void queue_sign(uint8_t *smem, int tid, const QueueArgs &q, const ItemRefs &r, uint32_t inst, int ctr,
                            uint32_t item) {
     using S = Set<SET>;
-    const uint8_t *esk = ops.sg_esk + (size_t)(inst % ops.sg_nkeys) * S::esk;
-    sign_hash_cta<SET, Q_NT>(smem, tid, esk, ops.sg_msg + (size_t)inst * ops.sg_mlen, ops.sg_mlen, ctr);
-    const bool ok = sign_attempt<SET, Q_NT>(smem, tid, esk);
+    constexpr int NT = QueueCfg<SET, MAYO_B200_OP_SIGN>::NT;
+    sign_hash_cta<SET, NT>(smem, tid, r.key, r.msg, r.mlen, ctr);
+    const bool ok = sign_attempt<SET, NT>(smem, tid, r.key);
     if (ok || ctr >= 254) {
         // success, or the 255th rejection: the reference emits the last attempt (x = r)
-        sign_write<SET, Q_NT>(smem, tid, esk, ops.sg_sig + (size_t)inst * S::sig);
+        sign_write<SET, NT>(smem, tid, r.key, q.ops.sg_sig + (size_t)inst * S::sig);
     } else if (tid == 0) {
         queue_push(q, (item & ~(0xFFu << 20)) | ((uint32_t)(ctr + 1) << 20));
     }
 }
 
-template <int SET>
-__device__ void queue_verify(uint8_t *smem, int tid, const QueueOps &ops, uint32_t inst) {
+template <int SET, int OP>
+__global__ void __launch_bounds__(QueueCfg<SET, OP>::NT, QueueFit<SET, OP>::MINB) queue_kernel(const QueueArgs q) {
     using S = Set<SET>;
-    const uint8_t *epk = ops.vf_epk + (size_t)(inst % ops.vf_nkeys) * S::epk;
-    verify_instance<SET, Q_NCV>(smem, tid, epk, ops.vf_msg + (size_t)inst * ops.vf_mlen, ops.vf_mlen,
-                                ops.vf_sig + (size_t)inst * S::sig, ops.vf_res + inst);
-}
-
-template <int SET>
-__device__ __forceinline__ void queue_dispatch(uint8_t *smem, int tid, const QueueArgs &q, uint32_t op, uint32_t inst,
-                                               int ctr, uint32_t item, uint8_t *scratch) {
-    const QueueOps &ops = q.ops[SET == 1 ? 0 : SET == 2 ? 1 : SET == 3 ? 2 : 3];
-    if (op == MAYO_B200_OP_KEYPAIR) queue_keypair<SET>(smem, tid, ops, inst, scratch);
-    else if (op == MAYO_B200_OP_SIGN) queue_sign<SET>(smem, tid, q, ops, inst, ctr, item);
-    else queue_verify<SET>(smem, tid, ops, inst);
-}
-
-__global__ void __launch_bounds__(Q_NT) queue_kernel(const QueueArgs q) {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint32_t s_item;
     const int tid = threadIdx.x;
-    uint8_t *scratch = q.scratch + (size_t)blockIdx.x * q.scratch_stride;
     for (;;) {
         if (tid == 0) s_item = queue_pop(q);
         __syncthreads();
         const uint32_t item = s_item;
         __syncthreads();
         if (item == Q_STOP) break;
-        const uint32_t op = item >> 30, si = (item >> 28) & 3, inst = item & 0xFFFFF;
-        const int ctr = (int)((item >> 20) & 0xFF);
-        switch (si) {
-            case 0: queue_dispatch<1>(smem, tid, q, op, inst, ctr, item, scratch); break;
-            case 1: queue_dispatch<2>(smem, tid, q, op, inst, ctr, item, scratch); break;
-            case 2: queue_dispatch<3>(smem, tid, q, op, inst, ctr, item, scratch); break;
-            default: queue_dispatch<5>(smem, tid, q, op, inst, ctr, item, scratch); break;
+        const uint32_t inst = item & 0xFFFFF;
+        const ItemRefs r = queue_refs<SET, OP>(q.ops, inst);
+        if (!r.ok) {
+            if (tid == 0) queue_error(q.ctrl, MAYO_B200_QUEUE_ERR_OPERAND);
+        } else if constexpr (OP == MAYO_B200_OP_KEYPAIR) {
+            queue_keypair<SET>(smem, tid, q.ops, inst, q.scratch + (size_t)blockIdx.x * q.scratch_stride);
+        } else if constexpr (OP == MAYO_B200_OP_SIGN) {
+            queue_sign<SET>(smem, tid, q, r, inst, (int)((item >> 20) & 0xFF), item);
+        } else {
+            verify_instance<SET, VerifyCfg<SET>::NC>(smem, tid, r.key, r.msg, r.mlen,
+                                                     q.ops.vf_sig + (size_t)inst * S::sig, q.ops.vf_res + inst);
         }
         __syncthreads();
         if (tid == 0) {
@@ -197,77 +255,276 @@ __global__ void __launch_bounds__(Q_NT) queue_kernel(const QueueArgs q) {
     }
 }
 
-// Queue reset: slots [0, n) <- items, [n, capacity) <- empty, counters <- (0, n, 0, 0, 0).
-__global__ void queue_reset_kernel(uint32_t *slots, const uint32_t *items, uint32_t n, uint32_t capacity,
-                                   uint32_t *ctrl) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < capacity) slots[i] = i < n ? items[i] : Q_EMPTY;
-    if (i < 8) ctrl[i] = i == 1 ? n : 0u;
+// Every bucket's slots <- empty, control words <- 0.
+constexpr int Q_CTRL_TOTAL = (Q_BUCKETS + 1) * Q_CTRL_WORDS;
+__global__ void queue_fill_kernel(uint32_t *slots, size_t nslots, uint32_t *ctrl) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nslots) slots[i] = Q_EMPTY;
+    if (i < Q_CTRL_TOTAL) ctrl[i] = 0u;
 }
 
-size_t queue_smem_bytes() {
-    size_t m = 0;
-    const size_t t[4] = {QueueLayout<1>::total_raw, QueueLayout<2>::total_raw, QueueLayout<3>::total_raw,
-                         QueueLayout<5>::total_raw};
-    for (size_t x : t) m = x > m ? x : m;
-    return pad16(m);
+// Stable partition of items[0, n) into the 12 (set, op) buckets (one CTA: per 1024-item chunk,
+// warp ballots give each item's rank within its warp and bucket, a scan over the warps gives the
+// warp's offset).  Items of a bucket without a kernel (`active` bit clear) are dropped with an
+// operand error in that bucket's control words, items with op 3 likewise in block 12.  n_dev,
+// when given, lowers n.
+constexpr int Q_PART_NT = 1024;
+__global__ void __launch_bounds__(Q_PART_NT) queue_partition_kernel(const uint32_t *items, uint32_t n,
+                                                                    const uint32_t *n_dev, uint32_t *slots,
+                                                                    uint32_t capacity, uint32_t *ctrl,
+                                                                    uint32_t active) {
+    __shared__ uint32_t s_warp[Q_PART_NT / 32][Q_BUCKETS + 1];
+    __shared__ uint32_t s_base[Q_BUCKETS + 1];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (n_dev) {
+        const uint32_t nd = *n_dev;
+        n = nd < n ? nd : n;
+    }
+    if (tid <= Q_BUCKETS) s_base[tid] = 0;
+    __syncthreads();
+    for (uint32_t start = 0; start < n; start += Q_PART_NT) {
+        const uint32_t i = start + tid;
+        const uint32_t it = i < n ? items[i] : 0u;
+        const uint32_t op = it >> 30;
+        const int b = i >= n ? -1 : (op == 3 ? Q_BUCKETS : (int)(((it >> 28) & 3) * 3 + op));
+        uint32_t rank = 0;
+#pragma unroll
+        for (int k = 0; k <= Q_BUCKETS; k++) {
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, b == k);
+            if (b == k) rank = __popc(bal & ((1u << lane) - 1u));
+            if (lane == 0) s_warp[warp][k] = __popc(bal);
+        }
+        __syncthreads();
+        if (tid <= Q_BUCKETS) {
+            uint32_t acc = s_base[tid];
+            for (int w = 0; w < Q_PART_NT / 32; w++) {
+                const uint32_t c = s_warp[w][tid];
+                s_warp[w][tid] = acc;
+                acc += c;
+            }
+            s_base[tid] = acc;
+        }
+        __syncthreads();
+        if (b >= 0 && b < Q_BUCKETS && ((active >> b) & 1u)) {
+            const uint32_t pos = s_warp[warp][b] + rank;
+            if (pos < capacity) slots[(size_t)b * capacity + pos] = it;
+        }
+        __syncthreads();
+    }
+    if (tid <= Q_BUCKETS) {
+        uint32_t *c = ctrl + tid * Q_CTRL_WORDS;
+        const uint32_t cnt = s_base[tid];
+        if (tid == Q_BUCKETS || !((active >> tid) & 1u)) {
+            c[0] = cnt;  // dropped
+            if (cnt) c[3] = MAYO_B200_QUEUE_ERR_OPERAND;
+        } else {
+            c[1] = cnt < capacity ? cnt : capacity;
+            if (cnt > capacity) c[3] = MAYO_B200_QUEUE_ERR_FULL;
+        }
+    }
 }
 
-size_t queue_scratch_stride() { return pad16((size_t)Set<5>::p + 16); }
+// ---- host side ----
+template <int SET, int OP>
+int bucket_ctas_per_sm() {
+    using QC = QueueCfg<SET, OP>;
+    if (!set_smem_attr(queue_kernel<SET, OP>, QC::smem)) return 0;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, queue_kernel<SET, OP>, QC::NT, QC::smem) != cudaSuccess)
+        return 0;
+    return per_sm;
+}
 
-int launch_queue(const QueueOps ops[4], const uint32_t *items, uint32_t n, uint32_t *slots, uint32_t capacity,
-                 uint32_t *ctrl, uint8_t *scratch, uint32_t ctas, uint32_t spin_limit, cudaStream_t st) {
-    if (n > capacity || ctas == 0) return ST_BAD_ARG;
-    queue_reset_kernel<<<(capacity + 255) / 256, 256, 0, st>>>(slots, items, n, capacity, ctrl);
-    const size_t smem = queue_smem_bytes();
-    if (!set_smem_attr(queue_kernel, smem)) return ST_CUDA;
-    QueueArgs q{};
-    for (int i = 0; i < 4; i++) q.ops[i] = ops[i];
-    q.items = slots;
-    q.capacity = capacity;
-    q.ctrl = ctrl;
-    q.scratch = scratch;
-    q.scratch_stride = queue_scratch_stride();
-    q.spin_limit = spin_limit;
-    queue_kernel<<<ctas, Q_NT, smem, st>>>(q);
+template <int SET, int OP>
+int bucket_launch(const QueueArgs &a, uint32_t ctas, cudaStream_t st) {
+    using QC = QueueCfg<SET, OP>;
+    if (!set_smem_attr(queue_kernel<SET, OP>, QC::smem)) return ST_CUDA;
+    queue_kernel<SET, OP><<<ctas, QC::NT, QC::smem, st>>>(a);
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+// Per bucket: residency (`launch` false) or launch.
+template <int SET, int OP>
+int bucket_call(bool launch, const QueueArgs *a, uint32_t ctas, cudaStream_t st) {
+    return launch ? bucket_launch<SET, OP>(*a, ctas, st) : bucket_ctas_per_sm<SET, OP>();
+}
+
+template <int SET>
+int bucket_call_op(int op, bool launch, const QueueArgs *a, uint32_t ctas, cudaStream_t st) {
+    switch (op) {
+        case MAYO_B200_OP_KEYPAIR: return bucket_call<SET, MAYO_B200_OP_KEYPAIR>(launch, a, ctas, st);
+        case MAYO_B200_OP_SIGN: return bucket_call<SET, MAYO_B200_OP_SIGN>(launch, a, ctas, st);
+        default: return bucket_call<SET, MAYO_B200_OP_VERIFY>(launch, a, ctas, st);
+    }
+}
+
+int bucket_dispatch(int b, bool launch, const QueueArgs *a = nullptr, uint32_t ctas = 0, cudaStream_t st = nullptr) {
+    const int si = b / 3, op = b % 3;
+    switch (si) {
+        case 0: return bucket_call_op<1>(op, launch, a, ctas, st);
+        case 1: return bucket_call_op<2>(op, launch, a, ctas, st);
+        case 2: return bucket_call_op<3>(op, launch, a, ctas, st);
+        default: return bucket_call_op<5>(op, launch, a, ctas, st);
+    }
+}
+
+size_t keypair_scratch(int si) {
+    switch (si) {
+        case 0: return QueueCfg<1, MAYO_B200_OP_KEYPAIR>::scratch;
+        case 1: return QueueCfg<2, MAYO_B200_OP_KEYPAIR>::scratch;
+        case 2: return QueueCfg<3, MAYO_B200_OP_KEYPAIR>::scratch;
+        default: return QueueCfg<5, MAYO_B200_OP_KEYPAIR>::scratch;
+    }
+}
+
+// Streams and events the kernels fork onto, per host thread and device (created on the first
+// call, outside any graph capture, and kept for the life of the thread).
+struct ForkSet {
+    bool ready = false;
+    cudaStream_t s[Q_BUCKETS];
+    cudaEvent_t fork, join[Q_BUCKETS];
+};
+constexpr int Q_MAX_DEVICES = 64;
+thread_local ForkSet tl_fork[Q_MAX_DEVICES];
+
+ForkSet *fork_set(int dev) {
+    if (dev < 0 || dev >= Q_MAX_DEVICES) return nullptr;
+    ForkSet &f = tl_fork[dev];
+    if (!f.ready) {
+        for (int i = 0; i < Q_BUCKETS; i++)
+            if (cudaStreamCreateWithFlags(&f.s[i], cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&f.join[i], cudaEventDisableTiming) != cudaSuccess)
+                return nullptr;
+        if (cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+        f.ready = true;
+    }
+    return &f;
 }
 
 }  // namespace mayo
 
 // ---- C-ABI ----
 namespace {
-constexpr size_t kCtrlBytes = 256;
+constexpr size_t kCtrlBytes = 1024;
+static_assert(mayo::Q_CTRL_TOTAL * 4 <= kCtrlBytes, "control words");
+// Default launch order: the buckets with the longest items first, so the short ones fill the
+// tails (measured per-item times on B200, longest first).
+constexpr uint8_t kDefaultOrder[mayo::Q_BUCKETS] = {9, 10, 11, 6, 7, 8, 0, 3, 1, 2, 4, 5};
+
 size_t slots_bytes(uint32_t capacity) { return (((size_t)capacity * 4) + 255) / 256 * 256; }
+
+int device_sms(int *dev) {
+    if (cudaGetDevice(dev) != cudaSuccess) return 0;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, *dev) != cudaSuccess) return 0;
+    return sms;
+}
+
+// Residency of every bucket's kernel and the byte offsets of the four keypair buckets' scratch
+// (after the control words and all slots), each sized for sms x its maximal residency.
+bool queue_layout(uint32_t capacity, uint32_t sms, int per_sm[mayo::Q_BUCKETS], size_t off[5]) {
+    for (int b = 0; b < mayo::Q_BUCKETS; b++) {
+        per_sm[b] = mayo::bucket_dispatch(b, false);
+        if (per_sm[b] <= 0) return false;
+    }
+    off[0] = kCtrlBytes + mayo::Q_BUCKETS * slots_bytes(capacity);
+    for (int si = 0; si < 4; si++)
+        off[si + 1] = off[si] + (size_t)sms * per_sm[si * 3 + MAYO_B200_OP_KEYPAIR] * mayo::keypair_scratch(si);
+    return true;
+}
+
+bool bucket_active(const mayo_b200_queue_ops &o, int op) {
+    if (op == MAYO_B200_OP_KEYPAIR) return o.kp_seed && o.kp_pk;
+    if (op == MAYO_B200_OP_SIGN) return o.sg_esk && o.sg_sig;
+    return o.vf_epk && o.vf_sig && o.vf_res;
+}
 }  // namespace
 
 extern "C" {
 
-MAYO_B200_API size_t mayo_b200_queue_mem_bytes(uint32_t capacity, uint32_t ctas) {
-    return kCtrlBytes + slots_bytes(capacity) + (size_t)ctas * mayo::queue_scratch_stride();
+MAYO_B200_API size_t mayo_b200_queue_mem_bytes(uint32_t capacity, uint32_t sms) {
+    int dev = 0;
+    const int dsms = device_sms(&dev);
+    if (!dsms) return 0;
+    if (!sms) sms = (uint32_t)dsms;
+    int per_sm[mayo::Q_BUCKETS];
+    size_t off[5];
+    if (!queue_layout(capacity, sms, per_sm, off)) return 0;
+    if (!mayo::fork_set(dev)) return 0;  // created here, before any graph capture
+    return off[4];
 }
 
-MAYO_B200_API int mayo_b200_queue_ctas_per_sm(void) {
-    int per_sm = 0;
-    const size_t smem = mayo::queue_smem_bytes();
-    if (!mayo::set_smem_attr(mayo::queue_kernel, smem)) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mayo::queue_kernel, mayo::Q_NT, smem) != cudaSuccess)
-        return 0;
-    return per_sm;
+MAYO_B200_API int mayo_b200_queue_ctas_per_sm(int set, int op) {
+    const int si = set == 1 ? 0 : set == 2 ? 1 : set == 3 ? 2 : set == 5 ? 3 : -1;
+    if (si < 0 || op < 0 || op > 2) return 0;
+    return mayo::bucket_dispatch(si * 3 + op, false);
 }
 
 MAYO_B200_API int mayo_b200_queue_run(const mayo_b200_queue_ops ops[4], const uint32_t *items, uint32_t n,
-                                      void *queue_mem, uint32_t capacity, uint32_t ctas, uint32_t spin_limit,
-                                      void *stream) {
-    if (!ops || !queue_mem || (n && !items) || n > capacity || ctas == 0 || capacity > (1u << 28))
+                                      const uint32_t *n_device, void *queue_mem, uint32_t capacity,
+                                      const mayo_b200_queue_shape *shape, uint32_t spin_limit, void *stream) {
+    using mayo::Q_BUCKETS;
+    if (!ops || !queue_mem || (n && !items) || n > capacity || capacity == 0 || capacity > (1u << 28))
         return MAYO_B200_ERR_ARG;
+    int dev = 0;
+    const int dsms = device_sms(&dev);
+    if (!dsms) return MAYO_B200_ERR_CUDA;
+    const uint32_t sms = shape && shape->sms ? shape->sms : (uint32_t)dsms;
+    int per_sm[Q_BUCKETS];
+    size_t off[5];
+    if (!queue_layout(capacity, sms, per_sm, off)) return MAYO_B200_ERR_CUDA;
+    uint8_t order[Q_BUCKETS];
+    for (int k = 0; k < Q_BUCKETS; k++) order[k] = kDefaultOrder[k];
+    if (shape) {
+        bool seen[Q_BUCKETS] = {}, perm = true;
+        for (int k = 0; k < Q_BUCKETS; k++) {
+            const uint8_t v = shape->launch_order[k];
+            if (v >= Q_BUCKETS || seen[v]) perm = false;
+            else seen[v] = true;
+        }
+        if (perm)
+            for (int k = 0; k < Q_BUCKETS; k++) order[k] = shape->launch_order[k];
+        for (int b = 0; b < Q_BUCKETS; b++)
+            if (shape->ctas_per_sm[b] > per_sm[b]) return MAYO_B200_ERR_ARG;
+    }
+    mayo::ForkSet *fs = mayo::fork_set(dev);
+    if (!fs) return MAYO_B200_ERR_CUDA;
+
     uint8_t *base = static_cast<uint8_t *>(queue_mem);
     uint32_t *ctrl = reinterpret_cast<uint32_t *>(base);
     uint32_t *slots = reinterpret_cast<uint32_t *>(base + kCtrlBytes);
-    uint8_t *scratch = base + kCtrlBytes + slots_bytes(capacity);
-    const int rc = mayo::launch_queue(ops, items, n, slots, capacity, ctrl, scratch, ctas,
-                                      spin_limit ? spin_limit : (1u << 24), reinterpret_cast<cudaStream_t>(stream));
-    return rc == mayo::ST_OK ? MAYO_B200_OK : (rc == mayo::ST_BAD_ARG ? MAYO_B200_ERR_ARG : MAYO_B200_ERR_CUDA);
+    const uint32_t cap_words = (uint32_t)(slots_bytes(capacity) / 4);  // each bucket's slots (padded)
+    const size_t nslots = (size_t)cap_words * Q_BUCKETS;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    uint32_t active = 0;
+    for (int b = 0; b < Q_BUCKETS; b++)
+        if (bucket_active(ops[b / 3], b % 3)) active |= 1u << b;
+
+    const size_t fill_n = nslots > (size_t)mayo::Q_CTRL_TOTAL ? nslots : (size_t)mayo::Q_CTRL_TOTAL;
+    mayo::queue_fill_kernel<<<(unsigned)((fill_n + 255) / 256), 256, 0, st>>>(slots, nslots, ctrl);
+    mayo::queue_partition_kernel<<<1, mayo::Q_PART_NT, 0, st>>>(items, n, n_device, slots, cap_words, ctrl, active);
+    if (cudaPeekAtLastError() != cudaSuccess || cudaEventRecord(fs->fork, st) != cudaSuccess) return MAYO_B200_ERR_CUDA;
+    int k = 0;
+    for (int j = 0; j < Q_BUCKETS; j++) {
+        const int b = order[j];
+        if (!(active & (1u << b))) continue;
+        cudaStream_t s = fs->s[k];
+        if (cudaStreamWaitEvent(s, fs->fork, 0) != cudaSuccess) return MAYO_B200_ERR_CUDA;
+        const uint32_t per = shape && shape->ctas_per_sm[b] ? shape->ctas_per_sm[b] : (uint32_t)per_sm[b];
+        mayo::QueueArgs a{};
+        a.ops = ops[b / 3];
+        a.slots = slots + (size_t)b * cap_words;
+        a.capacity = cap_words;
+        a.ctrl = ctrl + b * mayo::Q_CTRL_WORDS;
+        a.scratch = b % 3 == MAYO_B200_OP_KEYPAIR ? base + off[b / 3] : nullptr;
+        a.scratch_stride = mayo::keypair_scratch(b / 3);
+        a.spin_limit = spin_limit ? spin_limit : (1u << 24);
+        if (mayo::bucket_dispatch(b, true, &a, per * sms, s) != mayo::ST_OK) return MAYO_B200_ERR_CUDA;
+        if (cudaEventRecord(fs->join[k], s) != cudaSuccess || cudaStreamWaitEvent(st, fs->join[k], 0) != cudaSuccess)
+            return MAYO_B200_ERR_CUDA;
+        k++;
+    }
+    return MAYO_B200_OK;
 }
 
 }  // extern "C"

@@ -148,53 +148,88 @@ MAYO_B200_API int mayo_b200_verify_many(int set, const uint8_t *epk, size_t epk_
                                         size_t batch, void *stream);
 
 /* ---- Extension (no counterpart in the reference): persistent work queue ----
- * One launch of `ctas` resident CTAs drains a device queue of keypair / sign / verify items of
- * all four parameter sets.  A sign attempt with a singular system is re-enqueued with the next
- * attempt counter instead of being retried in place.  Every wait inside the kernel is bounded;
- * a queue that overflows or a wait that runs out ends the launch with an error code in the
- * queue's control words instead of hanging.  Results are byte-identical to the batched calls.
+ * A device queue of keypair / sign / verify items of all four parameter sets.  The mixed item
+ * array is partitioned on the device (stably) into 12 buckets, one per (set, op), each drained by
+ * its own persistent kernel shaped like the batched kernel for that (set, op) (their CTAs need
+ * 35-81 KB of shared memory, so one kernel for all would hold every set to the residency of the
+ * largest).  The kernels are launched on forked streams, so they share the SMs and fill each
+ * other's tails.  A sign attempt with a singular system is re-enqueued with the next attempt
+ * counter instead of being retried in place.  Every wait inside the kernels is bounded; an
+ * overflowing bucket, a wait that runs out or an item with a missing operand ends with an error
+ * code in the queue's control words instead of hanging or touching memory out of range.
+ * Results are byte-identical to the batched calls.
  *
  * Operands per parameter set (device pointers; an op's pointers may be NULL if no item uses it):
- *   keypair  instance i: seed = kp_seed + i*sk_bytes  -> pk at kp_pk + i*pk_bytes
- *   sign     instance i: key = sg_esk + (i % sg_nkeys)*esk_bytes, message sg_msg + i*sg_mlen
- *            (sg_mlen bytes) -> signature at sg_sig + i*sig_bytes
- *   verify   instance i: key = vf_epk + (i % vf_nkeys)*epk_bytes, message vf_msg + i*vf_mlen,
+ *   keypair  instance i < kp_count: seed kp_seed + i*sk_bytes -> pk at kp_pk + i*pk_bytes
+ *   sign     instance i < sg_count: key sg_esk + K*esk_bytes with K = sg_key[i] (or i % sg_nkeys
+ *            when sg_key is NULL); message sg_msg + sg_msg_off[i] of sg_msg_len[i] bytes (or
+ *            sg_msg + i*sg_mlen of sg_mlen bytes when they are NULL) -> signature sg_sig + i*sig_bytes
+ *   verify   instance i < vf_count: key vf_epk + K*epk_bytes likewise; message likewise;
  *            signature vf_sig + i*sig_bytes -> result byte vf_res[i] (0 accept, 1 reject)
- * Queue memory (mayo_b200_queue_mem_bytes bytes, device, caller-allocated): control words at
- * offset 0 (uint32: [0] tickets taken, [1] items published, [2] items finished, [3] error,
- * [4] re-enqueued signs), then the slots, then per-CTA scratch. */
+ * Bucket b = 3 * (set index: MAYO_1, 2, 3, 5 -> 0..3) + op.  Queue memory
+ * (mayo_b200_queue_mem_bytes bytes, device, caller-allocated): control words at offset 0, 16
+ * uint32 per bucket (bucket b at word 16*b): [0] tickets taken, [1] items published, [2] items
+ * finished, [3] error, [4] re-enqueued signs; block 12 counts items with an invalid op in [0]; a
+ * bucket whose op has no operands counts its dropped items in [0].  Then the slots (capacity per
+ * bucket), then the keypair buckets' per-CTA scratch. */
 enum { MAYO_B200_OP_KEYPAIR = 0, MAYO_B200_OP_SIGN = 1, MAYO_B200_OP_VERIFY = 2 };
-enum { MAYO_B200_QUEUE_OK = 0, MAYO_B200_QUEUE_ERR_FULL = 1, MAYO_B200_QUEUE_ERR_TIMEOUT = 2 };
+enum {
+    MAYO_B200_QUEUE_OK = 0,
+    MAYO_B200_QUEUE_ERR_FULL = 1,    /* more re-enqueued signs than slots */
+    MAYO_B200_QUEUE_ERR_TIMEOUT = 2, /* a wait ran past spin_limit */
+    MAYO_B200_QUEUE_ERR_OPERAND = 3  /* an item's instance, key index or operand is missing (item skipped) */
+};
 typedef struct mayo_b200_queue_ops {
     const uint8_t *kp_seed;
     uint8_t *kp_pk;
+    uint32_t kp_count;
     const uint8_t *sg_esk;
     uint32_t sg_nkeys;
+    const uint32_t *sg_key;
     const uint8_t *sg_msg;
+    const uint64_t *sg_msg_off;
+    const uint32_t *sg_msg_len;
     uint32_t sg_mlen;
     uint8_t *sg_sig;
+    uint32_t sg_count;
     const uint8_t *vf_epk;
     uint32_t vf_nkeys;
+    const uint32_t *vf_key;
     const uint8_t *vf_msg;
+    const uint64_t *vf_msg_off;
+    const uint32_t *vf_msg_len;
     uint32_t vf_mlen;
     const uint8_t *vf_sig;
     uint8_t *vf_res;
+    uint32_t vf_count;
 } mayo_b200_queue_ops;
+/* Launch shape.  sms: SMs the queue memory was sized for (0 = all SMs of the device); per
+ * bucket, ctas_per_sm (0 = the most that fit, at most mayo_b200_queue_ctas_per_sm) and the order
+ * in which the bucket kernels are launched (launch_order must be a permutation of 0..11, else the
+ * default: the buckets with the longest items first). */
+typedef struct mayo_b200_queue_shape {
+    uint32_t sms;
+    uint8_t ctas_per_sm[12];
+    uint8_t launch_order[12];
+} mayo_b200_queue_shape;
 /* Work item: op (MAYO_B200_OP_*), parameter set (1, 2, 3, 5), instance index < 2^20. */
 static inline uint32_t mayo_b200_queue_item(int op, int set, uint32_t instance) {
     const uint32_t si = set == 1 ? 0u : set == 2 ? 1u : set == 3 ? 2u : 3u;
     return ((uint32_t)op << 30) | (si << 28) | (instance & 0xFFFFFu);
 }
-/* Device bytes of queue memory for `capacity` slots and `ctas` resident CTAs. */
-MAYO_B200_API size_t mayo_b200_queue_mem_bytes(uint32_t capacity, uint32_t ctas);
-/* Resident CTAs per SM the queue kernel can hold on the current device (0 on error). */
-MAYO_B200_API int mayo_b200_queue_ctas_per_sm(void);
-/* Reset the queue to items[0..n) (device array) and run it to completion on `stream`.
- * capacity >= n; room beyond n holds re-enqueued signs (n + n/8 + 64 is ample).  Asynchronous;
- * graph-capturable (no allocation, no host synchronisation).  spin_limit 0 = default. */
+/* Device bytes of queue memory for `capacity` slots per bucket on `sms` SMs (0 = all); 0 on error. */
+MAYO_B200_API size_t mayo_b200_queue_mem_bytes(uint32_t capacity, uint32_t sms);
+/* Resident CTAs per SM of the queue kernel for (set, op) on the current device (0 on error). */
+MAYO_B200_API int mayo_b200_queue_ctas_per_sm(int set, int op);
+/* Reset the queue to items[0..n) (device array; when n_device is not NULL the count is
+ * min(*n_device, n), read on the device, so a captured graph can be replayed with a varying
+ * count) and run it to completion on `stream`.  capacity >= n; room beyond a bucket's items
+ * holds its re-enqueued signs (n + n/8 + 64 is ample).  shape NULL = defaults.  Asynchronous;
+ * graph-capturable (no allocation, no host synchronisation) once a first call on this host
+ * thread and device has returned.  spin_limit 0 = default. */
 MAYO_B200_API int mayo_b200_queue_run(const mayo_b200_queue_ops ops[4], const uint32_t *items, uint32_t n,
-                                      void *queue_mem, uint32_t capacity, uint32_t ctas, uint32_t spin_limit,
-                                      void *stream);
+                                      const uint32_t *n_device, void *queue_mem, uint32_t capacity,
+                                      const mayo_b200_queue_shape *shape, uint32_t spin_limit, void *stream);
 
 /* ---- Sign without caller workspace.  No counterpart in the reference API. ----
  * For callers that cannot allocate device memory (a service whose device-memory budget is

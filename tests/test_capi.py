@@ -72,3 +72,32 @@ def test_python_mirror_has_reference_names():
     m = M.Mayo(1)
     for r in ref:
         assert callable(getattr(m, r))
+
+
+def test_queue_structs_match_header(tmp_path):
+    """The ctypes mirrors of mayo_b200_queue_ops / _shape have the C layout (offsets, size)."""
+    from cumayo_b200 import queue as Q
+    structs = {"mayo_b200_queue_ops": Q._QueueOps, "mayo_b200_queue_shape": Q._QueueShape}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', f'#include "{HEADER}"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0; }")
+    src, exe = tmp_path / "layout.c", tmp_path / "layout"
+    src.write_text("\n".join(lines))
+    subprocess.run(["gcc", "-std=c99", "-o", str(exe), str(src)], check=True)
+    got = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    for line in filter(None, got):
+        cname, f, v = line.split()
+        py = structs[cname]
+        want = ctypes.sizeof(py) if f == "size" else getattr(py, f).offset
+        assert int(v) == want, (cname, f)
+
+
+def test_queue_item_encoding():
+    from cumayo_b200 import queue as Q
+    assert Q.item(Q.OP_VERIFY, 5, 0xABCDE) == (2 << 30) | (3 << 28) | 0xABCDE
+    assert Q.item(Q.OP_KEYPAIR, 1, 1 << 20) == 0  # instance wraps at 20 bits, as the C helper
+    arr = Q.items_array([(Q.OP_SIGN, 3, 7)])
+    assert arr.dtype.name == "uint32" and int(arr[0]) == (1 << 30) | (2 << 28) | 7
