@@ -32,6 +32,18 @@ if ROOT not in sys.path:
 
 METRIC = "sign/s and verify/s per B200 (MAYO_1/2/3/5), byte-exact; serving p50/p99 vs plain"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def _hbm_peak() -> tuple[float, str]:
+    """Measured copy bandwidth of this GPU pool (MEASURED_PEAKS.json), else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback"
+
+
+HBM_PEAK_GBS, HBM_PEAK_SRC = _hbm_peak()
 LOP3_LANE_OPS_PER_CLK_SM = 64  # measured on this pool's B200 (profiles/int_pipes_b200.md)
 A128 = lambda x: (x + 127) // 128 * 128  # noqa: E731
 
@@ -44,6 +56,7 @@ WORKLOADS = {
     "c3-3": dict(set=3, batch=16384, kind="distinct_verify", mlen=(32, 32)),
     "c3-5": dict(set=5, batch=16384, kind="distinct_verify", mlen=(32, 32)),
     "c4": dict(set=0, batch=262144, kind="mixed_queue", mlen=(32, 32)),
+    "c5": dict(set=0, batch=16384, kind="serving", mlen=(32, 256)),
 }
 
 PARAMS = {1: (86, 78, 8, 10), 2: (81, 64, 17, 4), 3: (118, 108, 10, 11), 5: (154, 142, 12, 12)}
@@ -444,10 +457,10 @@ def run_ours(args, dist: Dist):
                                        "LOP3 issue rate 64 lane-ops/clk/SM x 148 SMs x median SM clock"},
         "roofline_hbm": {"bound": "hbm", "kernel": f"{dom} ({args.workload})",
                          "achieved": round(hbm_bytes[dom] / (phase_ms[dom] / 1e3) / 1e9, 2),
-                         "peak": 6550.1, "unit": "GB/s",
-                         "frac": round(hbm_bytes[dom] / (phase_ms[dom] / 1e3) / 1e9 / 6550.1, 5), "traffic": None,
+                         "peak": HBM_PEAK_GBS, "unit": "GB/s",
+                         "frac": round(hbm_bytes[dom] / (phase_ms[dom] / 1e3) / 1e9 / HBM_PEAK_GBS, 5), "traffic": None,
                          "definition": "algorithmic bytes the kernel must move from HBM per launch / kernel time; "
-                                       "peak = MEASURED_PEAKS hbm_gbs (copy)"},
+                                       f"peak = copy bandwidth ({HBM_PEAK_SRC})"},
         "e2e": {"value": round(ops_per_step * dist.world / (e2e_ms / args.steps / 1e3), 1), "unit": "ops/s",
                 "h2d_bytes_per_step": int(h2d_bytes), "d2h_bytes_per_step": int(d2h_bytes)},
         "gpu_launches": launches_per_step * args.steps,
@@ -921,6 +934,214 @@ def run_reference_pool(args, dist: Dist, path: str):
     return out
 
 
+# ---------------------------------------------------------------------------------------------
+# C5: serving (open-loop Poisson arrivals, continuous batching, resident key cache)
+# ---------------------------------------------------------------------------------------------
+SERVE_MIX = {1: 0.4, 2: 0.3, 3: 0.2, 5: 0.1}
+SERVE_KEYS = {1: 1638, 2: 1229, 3: 819, 5: 410}  # 4096 resident keys at the set mix
+
+
+def serving_stream(seed: int, rate: float, n: int, n_tmpl: dict, tmpl_base: dict):
+    """n requests at `rate`/s: ChaCha20-driven exponential gaps; 70 % verify / 30 % sign; sets
+    40/30/20/10; a uniform request template of the set; 1 % of verifies carry a corrupted
+    signature.  Returns (arrivals, op, template index, corrupted)."""
+    from cumayo_b200 import queue as Q
+    from cumayo_b200 import serving as SV
+    arr = SV.poisson_arrivals(rate, n, (b"c5-arrivals-%d-%d" % (seed, int(rate))).ljust(32, b"\0")[:32])
+    u = chacha((b"c5-requests-%d-%d" % (seed, int(rate))).ljust(32, b"\0")[:32], 16 * n).view(np.uint32).reshape(n, 4)
+    f = (u.astype(np.float64) + 0.5) / 2.0 ** 32
+    op = np.where(f[:, 0] < 0.7, Q.OP_VERIFY, Q.OP_SIGN).astype(np.uint8)
+    cum = np.cumsum([SERVE_MIX[s] for s in (1, 2, 3, 5)])
+    set_id = np.array([1, 2, 3, 5])[np.searchsorted(cum, f[:, 1] * cum[-1], side="right").clip(0, 3)]
+    base = np.array([tmpl_base[s] for s in set_id])
+    cnt = np.array([n_tmpl[s] for s in set_id])
+    tidx = base + (u[:, 2] % cnt.astype(np.uint32)).astype(np.int64)
+    bad = (op == Q.OP_VERIFY) & (f[:, 3] < 0.01)
+    return arr, op, tidx, bad
+
+
+def run_serving(args, dist: Dist):
+    import torch
+
+    import cumayo_b200 as M
+    from cumayo_b200 import queue as Q
+    from cumayo_b200 import serving as SV
+    dev = torch.device("cuda", dist.local)
+    torch.cuda.set_device(dev)
+    st = torch.cuda.current_stream()
+    seed = 1 + dist.rank
+    max_msg, budget = 256, 60 << 30
+    max_batch = args.batch or WORKLOADS["c5"]["batch"]
+    sets = (1, 2, 3, 5)
+
+    # keys (all resident: 4096 keys ~ 2 GB of esk + epk, far inside the budget)
+    seeds = {s: seeds_for(seed * 100 + s, SERVE_KEYS[s], M.sizes(s).sk_bytes) for s in sets}
+    cache = SV.KeyCache(seeds, SV.KeyCache.capacity_for_budget(budget // 2, SERVE_KEYS), device=dev)
+    server = SV.Server(cache, max_batch=max_batch, inflight=2, max_msg=max_msg, budget_bytes=budget)
+    for s in sets:  # load every key once, outside the timed runs
+        _, su = cache.acquire(s, np.arange(SERVE_KEYS[s]), st)
+        cache.release(s, su)
+    torch.cuda.synchronize()
+
+    # request templates: per set 4096 (key, message) pairs and their signatures, computed by the
+    # server itself; a sample is checked against the plain batched sign_many below
+    n_tmpl = {s: 4096 for s in sets}
+    tmpl_base, tset, tkey, tmlen, tmsg = {}, [], [], [], []
+    b = 0
+    for s in sets:
+        tmpl_base[s] = b
+        b += n_tmpl[s]
+        raw = chacha((b"c5-templates-%d-%d" % (seed, s)).ljust(32, b"\0")[:32], 8 * n_tmpl[s]).view(np.uint32)
+        tset.append(np.full(n_tmpl[s], s, np.int64))
+        tkey.append((raw[0::2] % SERVE_KEYS[s]).astype(np.int64))
+        tmlen.append((32 + raw[1::2] % (max_msg - 31)).astype(np.uint32))
+        tmsg.append(chacha((b"c5-msgs-%d-%d" % (seed, s)).ljust(32, b"\0")[:32], n_tmpl[s] * max_msg)
+                    .reshape(n_tmpl[s], max_msg))
+    tset, tkey, tmlen, tmsg = (np.concatenate(x) for x in (tset, tkey, tmlen, tmsg))
+    T = tset.size
+    tset = tset.astype(np.uint8)
+    tsig = np.zeros((T, SV.MAX_SIG), np.uint8)
+    ROW_MSG, ROW_SIG = np.uint64(max_msg), np.uint64(SV.MAX_SIG)
+
+    # template signatures, written by the server straight into tsig
+    for lo in range(0, T, max_batch):
+        rows = np.arange(lo, min(T, lo + max_batch), dtype=np.uint64)
+        r = SV.make_requests(np.full(rows.size, Q.OP_SIGN, np.uint8), tset[rows], tkey[rows], tmlen[rows],
+                             tmsg.ctypes.data + rows * ROW_MSG, 0, tsig.ctypes.data + rows * ROW_SIG)
+        server.launch(r, tag=(lo, lo + rows.size))
+        server.drain()
+    server.check_queue()
+    tbad = tsig.copy()
+    tbad[:, 7] ^= 0x40  # every template's signature, corrupted
+    # cross-check: 64 templates per set through the plain batched path (gathered keys)
+    plain_bad = 0
+    for s in sets:
+        z = M.sizes(s)
+        rows = tmpl_base[s] + np.arange(64)
+        esk = cache.esk[s].view(-1, z.esk_bytes)[torch.from_numpy(cache.tables[s].slot_of[tkey[rows]]).to(dev)]
+        msgs = torch.from_numpy(tmsg[rows].copy()).to(dev)
+        lens = torch.from_numpy(tmlen[rows].astype(np.int32)).to(dev)
+        offs = torch.arange(64, dtype=torch.int64, device=dev) * max_msg
+        sig = torch.zeros(64 * z.sig_bytes, dtype=torch.uint8, device=dev)
+        ws = torch.zeros(64 * M.Mayo(s).sign_ws_bytes(), dtype=torch.uint8, device=dev)
+        M.Mayo(s).sign_many(esk.reshape(-1), msgs.reshape(-1), sig, ws, 64, esk_stride=z.esk_bytes, msg_off=offs,
+                            msg_len=lens, stream=st)
+        plain_bad += int((sig.cpu().numpy().reshape(64, z.sig_bytes) != tsig[rows, : z.sig_bytes]).any(1).sum())
+
+    mismatches = [plain_bad]
+
+    def runner(arr, op, tidx, bad):
+        def fetch(lo, hi):
+            t = tidx[lo:hi].astype(np.uint64)
+            out = np.empty((hi - lo, SV.MAX_SIG), np.uint8)
+            sig_base = np.where(bad[lo:hi], np.uint64(tbad.ctypes.data), np.uint64(tsig.ctypes.data))
+            r = SV.make_requests(op[lo:hi], tset[t], tkey[t], tmlen[t], tmsg.ctypes.data + t * ROW_MSG,
+                                 sig_base + t * ROW_SIG, out.ctypes.data + np.arange(hi - lo, dtype=np.uint64) * ROW_SIG)
+            return r, out
+
+        def on_done(lo, hi, out):
+            t = tidx[lo:hi]
+            sg = op[lo:hi] == Q.OP_SIGN
+            nb = 0
+            for s_ in sets:
+                rows = np.flatnonzero(sg & (tset[t] == s_))
+                sb = M.sizes(s_).sig_bytes
+                nb += int((out[rows, :sb] != tsig[t[rows], :sb]).any(1).sum())
+            nb += int((out[: hi - lo][~sg, 0] != bad[lo:hi][~sg].astype(np.uint8)).sum())
+            mismatches[0] += nb
+
+        b0 = server.batches
+        lat, wall, bs = SV.run_open_loop(server, arr, fetch, on_done)
+        served_t = lat + arr
+        return lat, float(np.nanmax(served_t)), bs, server.batches - b0
+
+    # closed-loop batched peak through the same path (every request waiting from t = 0)
+    n_peak = max_batch * 12
+    arr, op, tidx, bad = serving_stream(seed, 1e12, n_peak, n_tmpl, tmpl_base)
+    arr[:] = 0.0
+    runner(arr, op, tidx, bad)  # warm-up
+    lat, span, bs, _ = runner(arr, op, tidx, bad)
+    peak = n_peak / span
+
+    # plain per-(set, op) batched launches of the same mix (one shared key per set, device inputs)
+    counts = {(s, o): int(((tset[tidx] == s) & (op == o)).sum()) for s in sets for o in (Q.OP_SIGN, Q.OP_VERIFY)}
+    plain_parts = []
+    for s in sets:
+        z = M.sizes(s)
+        esk, epk = expand_shared_key(M.Mayo(s), seeds[s][0], dev, st)
+        nmax = max(counts[(s, Q.OP_SIGN)], counts[(s, Q.OP_VERIFY)], 1)
+        msgs = torch.from_numpy(np.resize(tmsg[tmpl_base[s]: tmpl_base[s] + n_tmpl[s]], (nmax, max_msg))).to(dev)
+        lens = torch.from_numpy(np.resize(tmlen[tmpl_base[s]: tmpl_base[s] + n_tmpl[s]], nmax).astype(np.int32)).to(dev)
+        offs = torch.arange(nmax, dtype=torch.int64, device=dev) * max_msg
+        sig = torch.zeros(nmax * z.sig_bytes, dtype=torch.uint8, device=dev)
+        ws = torch.zeros(nmax * M.Mayo(s).sign_ws_bytes(), dtype=torch.uint8, device=dev)
+        res = torch.zeros(nmax, dtype=torch.uint8, device=dev)
+        plain_parts.append((M.Mayo(s), esk, epk, msgs, offs, lens, sig, ws, res, counts[(s, Q.OP_SIGN)],
+                            counts[(s, Q.OP_VERIFY)]))
+
+    def plain():
+        for m, esk, epk, msgs, offs, lens, sig, ws, res, ns, nv in plain_parts:
+            if ns:
+                m.sign_many(esk, msgs.reshape(-1), sig, ws, ns, msg_off=offs, msg_len=lens, stream=st)
+            if nv:
+                m.verify_many(epk, msgs.reshape(-1), sig, res, nv, msg_off=offs, msg_len=lens, stream=st)
+
+    plain()
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(st)
+    for _ in range(3):
+        plain()
+    p1.record(st)
+    torch.cuda.synchronize()
+    plain_peak = n_peak * 3 / (p0.elapsed_time(p1) / 1e3)
+
+    # open-loop sweep
+    target = 0.8 * peak
+    rates = sorted({5e4, 2e5, 5e5, 1e6, round(target, -3), round(0.9 * peak, -3), 2e6})
+    sweep, head = [], None
+    clocks = Clocks(dist.local)
+    clocks.start()
+    l0 = server.kernel_launches
+    for rate in rates:
+        n = int(min(rate * 0.5, 1.2e6))
+        arr, op, tidx, bad = serving_stream(seed, rate, n, n_tmpl, tmpl_base)
+        lat, span, bs, nb = runner(arr, op, tidx, bad)
+        row = dict(SV.latency_stats(lat), offered_per_s=rate, served_per_s=round(n / span, 1),
+                   batches=int(nb), mean_batch=round(float(bs.mean()), 1), max_batch=int(bs.max()))
+        sweep.append(row)
+        if rate == round(target, -3):
+            head = row
+    clk = clocks.stop()
+    mean_sig = sum(SERVE_MIX[s] * M.sizes(s).sig_bytes for s in sets)
+    bytes_in = 4 + 4 + 4 + float(tmlen.mean()) + 0.7 * mean_sig  # item, key slot, length, message, signature
+    bytes_out = 0.3 * mean_sig + 0.7
+    out = {
+        "metric": METRIC, "value": head["served_per_s"], "unit": "req/s", "n_gpus": dist.world,
+        "steps": len(rates), "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 (GF(16) bit-planes)", "data": "synthetic (seeded ChaCha20)",
+        "config": {"workload": "serving: open-loop Poisson arrivals, 70 % verify / 30 % sign, sets 40/30/20/10, "
+                               "4096 resident keys, continuous batching over the persistent queue",
+                   "max_batch": max_batch, "inflight_batches": 2, "msg_len": f"32..{max_msg} B",
+                   "key_cache_bytes": cache.nbytes(), "device_bytes": server.device_bytes, "budget_bytes": budget,
+                   "value": "requests/s served at an offered load of 0.8 x the closed-loop batched peak"},
+        "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"], "p999_ms": head["p999_ms"],
+        "offered_per_s": head["offered_per_s"],
+        "batched_peak_per_s": round(peak, 1), "plain_batched_peak_per_s": round(plain_peak, 1),
+        "sweep": sweep,
+        "e2e": {"value": head["served_per_s"], "unit": "req/s",
+                "h2d_bytes_per_step": int(bytes_in * head["n"] / max(head.get("batches", 1), 1)),
+                "d2h_bytes_per_step": int(bytes_out * head["n"] / max(head.get("batches", 1), 1)),
+                "note": "every number here is end to end (host request buffers in, host results out); "
+                        "a step is one admitted batch"},
+        "roofline": None,
+        "gpu_launches": server.kernel_launches - l0,
+        "clocks": clk,
+        "result_mismatches": mismatches[0],
+    }
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -943,7 +1164,12 @@ def main():
         return
     dist = Dist()
     try:
-        out = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
+        if args.impl == "reference":
+            out = run_reference(args, dist)
+        elif WORKLOADS[args.workload]["kind"] == "serving":
+            out = run_serving(args, dist)
+        else:
+            out = run_ours(args, dist)
     finally:
         dist.close()
     if dist.rank == 0:

@@ -13,14 +13,13 @@
 // and the CTAs of a kernel launched later take the SMs of one whose bucket has drained, so one
 // bucket's tail overlaps another's work.
 //
-// Inside a kernel each CTA takes the next item with an atomic ticket, runs it with the same
-// device functions as the batched kernels, and takes the next.  A sign attempt whose linear
-// system is singular is not retried in place: the CTA pushes (sign, ctr + 1) to the tail of its
-// bucket and moves on, so one rare rejection never holds a CTA back.  A bucket is drained when
-// every published item is finished (done == tail; `done` is read before `tail`, so a push from an
-// unfinished item can never be missed).  A CTA only ever waits for items held by CTAs of its own
-// kernel that are already running, so the kernels need not be co-resident.  Waits are bounded: a
-// ticket that stays unpublished past `spin_limit` sleeps sets an error code and ends the CTA.
+// Inside a kernel each CTA takes the next item (see queue_pop), runs it with the same device
+// functions as the batched kernels, and takes the next; a CTA that finds its bucket empty exits
+// at once and frees its SM for the other buckets' kernels.  A sign attempt whose linear system is singular is not retried in place: the CTA
+// pushes (sign, ctr + 1) to the tail of its bucket and goes on popping, so the item is served
+// either by that CTA or by another one still running.  No CTA waits for another kernel, so the
+// kernels need not be co-resident.  Every wait is bounded: past `spin_limit` it sets an error
+// code and ends the CTA.
 #include <cuda_runtime.h>
 
 #include "../../include/mayo_b200.h"
@@ -82,7 +81,7 @@ struct QueueArgs {
     QueueOps ops;
     uint32_t *slots;
     uint32_t capacity;
-    uint32_t *ctrl;  // [0] head ticket, [1] tail, [2] done, [3] error, [4] pushes
+    uint32_t *ctrl;  // [0] head, [1] tail, [2] done, [3] error, [4] pushes
     uint8_t *scratch;
     size_t scratch_stride;
     uint32_t spin_limit;
@@ -92,27 +91,50 @@ __device__ __forceinline__ uint32_t ld_volatile(const uint32_t *p) { return *rei
 
 __device__ __forceinline__ void queue_error(uint32_t *ctrl, uint32_t code) { atomicCAS(&ctrl[3], 0u, code); }
 
-__device__ uint32_t queue_pop(const QueueArgs &q) {
-    const uint32_t idx = atomicAdd(&q.ctrl[0], 1u);
-    for (uint32_t it = 0;; it++) {
-        if (idx < q.capacity) {
-            const uint32_t v = ld_volatile(&q.slots[idx]);
-            if (v != Q_EMPTY) {
-                __threadfence();
-                return v;
-            }
+// Take the next item.  Near the end of a bucket head moves by compare-and-swap and only while
+// head < tail, so no ticket is handed out past the published items and a CTA that finds its
+// bucket empty leaves at once, freeing its SM for the other buckets' kernels.  A sign re-enqueued
+// later is still served: the CTA that pushed it keeps popping, and it either takes the item
+// itself or finds it taken by another CTA.  While at least gridDim items remain, head moves by
+// atomicAdd (no retries under contention); such a ticket can overshoot the tail only if other
+// CTAs popped several times in between, and then it waits, as every ticket past the tail must,
+// for a push into its slot or for the bucket to drain (done == tail: `done` is read first, so a
+// push from an unfinished item cannot be missed).  Every wait is bounded by spin_limit.
+__device__ uint32_t queue_wait_slot(const QueueArgs &q, uint32_t h, uint32_t &it) {
+    for (;; it++) {
+        const uint32_t v = ld_volatile(&q.slots[h]);
+        if (v != Q_EMPTY) {
+            __threadfence();
+            return v;
         }
         const uint32_t done = ld_volatile(&q.ctrl[2]);
         __threadfence();
         const uint32_t tail = ld_volatile(&q.ctrl[1]);
-        if (idx >= tail && done == tail) return Q_STOP;  // drained: no unfinished item can push
-        // A ticket past the last slot can only end with the drain; a ticket inside the queue
-        // waits for its item to be published.  Both waits are bounded.
+        if (h >= tail && done == tail) return Q_STOP;  // drained: no unfinished item can push
         if (it >= q.spin_limit) {
             queue_error(q.ctrl, MAYO_B200_QUEUE_ERR_TIMEOUT);
             return Q_STOP;
         }
-        __nanosleep(200);
+        __nanosleep(100);
+    }
+}
+
+__device__ uint32_t queue_pop(const QueueArgs &q) {
+    uint32_t it = 0;
+    for (;;) {
+        const uint32_t h = ld_volatile(&q.ctrl[0]);
+        const uint32_t t = ld_volatile(&q.ctrl[1]);
+        const uint32_t lim = t < q.capacity ? t : q.capacity;
+        if (h >= lim) return Q_STOP;
+        if (lim - h >= gridDim.x) {
+            const uint32_t h2 = atomicAdd(&q.ctrl[0], 1u);
+            return h2 < q.capacity ? queue_wait_slot(q, h2, it) : Q_STOP;
+        }
+        if (atomicCAS(&q.ctrl[0], h, h + 1) == h) return queue_wait_slot(q, h, it);
+        if (++it >= q.spin_limit) {  // lost the race that many times
+            queue_error(q.ctrl, MAYO_B200_QUEUE_ERR_TIMEOUT);
+            return Q_STOP;
+        }
     }
 }
 
@@ -120,8 +142,7 @@ __device__ void queue_push(const QueueArgs &q, uint32_t item) {
     const uint32_t slot = atomicAdd(&q.ctrl[1], 1u);
     if (slot >= q.capacity) {
         queue_error(q.ctrl, MAYO_B200_QUEUE_ERR_FULL);
-        // the slot never becomes visible; count the item as finished so the queue still drains
-        atomicAdd(&q.ctrl[2], 1u);
+        atomicAdd(&q.ctrl[2], 1u);  // the item is dropped: count it as finished
         return;
     }
     atomicAdd(&q.ctrl[4], 1u);
@@ -377,27 +398,37 @@ size_t keypair_scratch(int si) {
     }
 }
 
-// Streams and events the kernels fork onto, per host thread and device (created on the first
-// call, outside any graph capture, and kept for the life of the thread).
+// Streams and events the kernels fork onto, per host thread, device and caller stream (created
+// on the first call, outside any graph capture, and kept for the life of the thread), so that
+// runs issued on different caller streams stay concurrent.  Past Q_FORK_SETS caller streams the
+// last set is shared: still correct (its streams keep the runs in issue order), only serialised.
 struct ForkSet {
-    bool ready = false;
+    int dev = -1;
+    cudaStream_t caller = nullptr;
     cudaStream_t s[Q_BUCKETS];
     cudaEvent_t fork, join[Q_BUCKETS];
 };
-constexpr int Q_MAX_DEVICES = 64;
-thread_local ForkSet tl_fork[Q_MAX_DEVICES];
+constexpr int Q_FORK_SETS = 16;
+thread_local ForkSet tl_fork[Q_FORK_SETS];
+thread_local int tl_fork_used = 0;
 
-ForkSet *fork_set(int dev) {
-    if (dev < 0 || dev >= Q_MAX_DEVICES) return nullptr;
-    ForkSet &f = tl_fork[dev];
-    if (!f.ready) {
-        for (int i = 0; i < Q_BUCKETS; i++)
-            if (cudaStreamCreateWithFlags(&f.s[i], cudaStreamNonBlocking) != cudaSuccess ||
-                cudaEventCreateWithFlags(&f.join[i], cudaEventDisableTiming) != cudaSuccess)
-                return nullptr;
-        if (cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming) != cudaSuccess) return nullptr;
-        f.ready = true;
+ForkSet *fork_set(int dev, cudaStream_t caller) {
+    for (int i = 0; i < tl_fork_used; i++)
+        if (tl_fork[i].dev == dev && tl_fork[i].caller == caller) return &tl_fork[i];
+    if (tl_fork_used == Q_FORK_SETS) {
+        for (int i = Q_FORK_SETS - 1; i >= 0; i--)
+            if (tl_fork[i].dev == dev) return &tl_fork[i];
+        return nullptr;
     }
+    ForkSet &f = tl_fork[tl_fork_used];
+    for (int i = 0; i < Q_BUCKETS; i++)
+        if (cudaStreamCreateWithFlags(&f.s[i], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&f.join[i], cudaEventDisableTiming) != cudaSuccess)
+            return nullptr;
+    if (cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+    f.dev = dev;
+    f.caller = caller;
+    tl_fork_used++;
     return &f;
 }
 
@@ -450,7 +481,6 @@ MAYO_B200_API size_t mayo_b200_queue_mem_bytes(uint32_t capacity, uint32_t sms) 
     int per_sm[mayo::Q_BUCKETS];
     size_t off[5];
     if (!queue_layout(capacity, sms, per_sm, off)) return 0;
-    if (!mayo::fork_set(dev)) return 0;  // created here, before any graph capture
     return off[4];
 }
 
@@ -487,7 +517,8 @@ MAYO_B200_API int mayo_b200_queue_run(const mayo_b200_queue_ops ops[4], const ui
         for (int b = 0; b < Q_BUCKETS; b++)
             if (shape->ctas_per_sm[b] > per_sm[b]) return MAYO_B200_ERR_ARG;
     }
-    mayo::ForkSet *fs = mayo::fork_set(dev);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    mayo::ForkSet *fs = mayo::fork_set(dev, st);
     if (!fs) return MAYO_B200_ERR_CUDA;
 
     uint8_t *base = static_cast<uint8_t *>(queue_mem);
@@ -495,7 +526,6 @@ MAYO_B200_API int mayo_b200_queue_run(const mayo_b200_queue_ops ops[4], const ui
     uint32_t *slots = reinterpret_cast<uint32_t *>(base + kCtrlBytes);
     const uint32_t cap_words = (uint32_t)(slots_bytes(capacity) / 4);  // each bucket's slots (padded)
     const size_t nslots = (size_t)cap_words * Q_BUCKETS;
-    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     uint32_t active = 0;
     for (int b = 0; b < Q_BUCKETS; b++)
         if (bucket_active(ops[b / 3], b % 3)) active |= 1u << b;

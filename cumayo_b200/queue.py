@@ -188,6 +188,15 @@ class Queue:
                                      _ptr(self.mem), self.capacity, ctypes.byref(shp), spin_limit, _stream(stream)),
                "queue_run")
 
+    def run_items(self, items_ptr: int, n: int, stream=None, spin_limit: int = 0) -> None:
+        """Run n items already on the device at `items_ptr` (e.g. inside a staged input buffer)."""
+        if n > self.capacity:
+            raise MayoError(f"{n} items exceed the queue capacity {self.capacity}")
+        L = _bind()
+        shp = self.shape.to_c()
+        _check(L.mayo_b200_queue_run(self._ops, items_ptr, n, None, _ptr(self.mem), self.capacity, ctypes.byref(shp),
+                                     spin_limit, _stream(stream)), "queue_run")
+
     def capture(self, device_count: bool = False) -> None:
         """Capture run() into a CUDA graph (replay with replay()).  With device_count the graph
         reads the item count from the device at each replay, up to the capacity."""
@@ -209,9 +218,10 @@ class Queue:
 
     def stats(self) -> dict:
         """Control words after a run (synchronises): totals over the buckets, the first error code,
-        per (set, op) bucket the same words, and the items dropped for an invalid op."""
+        per (set, op) bucket the same words ("taken" counts the items a bucket without operands
+        dropped), and the items dropped for an invalid op."""
         c = self.mem[:13 * 64].cpu().numpy().view(np.uint32).reshape(13, 16)
-        per = {(s, op): {"tickets": int(c[b, 0]), "published": int(c[b, 1]), "finished": int(c[b, 2]),
+        per = {(s, op): {"taken": int(c[b, 0]), "published": int(c[b, 1]), "finished": int(c[b, 2]),
                          "error": int(c[b, 3]), "requeued_signs": int(c[b, 4])}
                for b, (s, op) in enumerate(BUCKETS)}
         err = next((p["error"] for p in per.values() if p["error"]), int(c[12, 3]))

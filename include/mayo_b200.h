@@ -168,7 +168,7 @@ MAYO_B200_API int mayo_b200_verify_many(int set, const uint8_t *epk, size_t epk_
  *            signature vf_sig + i*sig_bytes -> result byte vf_res[i] (0 accept, 1 reject)
  * Bucket b = 3 * (set index: MAYO_1, 2, 3, 5 -> 0..3) + op.  Queue memory
  * (mayo_b200_queue_mem_bytes bytes, device, caller-allocated): control words at offset 0, 16
- * uint32 per bucket (bucket b at word 16*b): [0] tickets taken, [1] items published, [2] items
+ * uint32 per bucket (bucket b at word 16*b): [0] items taken, [1] items published, [2] items
  * finished, [3] error, [4] re-enqueued signs; block 12 counts items with an invalid op in [0]; a
  * bucket whose op has no operands counts its dropped items in [0].  Then the slots (capacity per
  * bucket), then the keypair buckets' per-CTA scratch. */
@@ -225,11 +225,55 @@ MAYO_B200_API int mayo_b200_queue_ctas_per_sm(int set, int op);
  * min(*n_device, n), read on the device, so a captured graph can be replayed with a varying
  * count) and run it to completion on `stream`.  capacity >= n; room beyond a bucket's items
  * holds its re-enqueued signs (n + n/8 + 64 is ample).  shape NULL = defaults.  Asynchronous;
- * graph-capturable (no allocation, no host synchronisation) once a first call on this host
- * thread and device has returned.  spin_limit 0 = default. */
+ * runs on different streams (with their own queue memory) overlap.  The first call from a host
+ * thread for a given stream creates the streams the bucket kernels fork onto; after that the
+ * call is graph-capturable (no allocation, no host synchronisation).  spin_limit 0 = default. */
 MAYO_B200_API int mayo_b200_queue_run(const mayo_b200_queue_ops ops[4], const uint32_t *items, uint32_t n,
                                       const uint32_t *n_device, void *queue_mem, uint32_t capacity,
                                       const mayo_b200_queue_shape *shape, uint32_t spin_limit, void *stream);
+
+/* ---- Extension (no counterpart in the reference): serving-batch staging (host code) ----
+ * A serving loop admits sign / verify requests whose messages, signatures and result buffers
+ * live in the caller's host memory.  mayo_b200_serve_pack copies one batch of them, in one pass,
+ * into a staging buffer laid out for the work queue (items, then per (set, op) group its key
+ * slots, message lengths, messages at a max_msg stride and, for verifies, signatures at the
+ * set's stride, every section 16-byte aligned); after the queue has run on the device copy of
+ * that buffer, mayo_b200_serve_unpack copies each request's signature (sig_bytes of its set) or
+ * verify result byte (0 accept, 1 reject) from the output staging buffer to its `out`.  The
+ * layout gives each group's offsets, from which the caller fills mayo_b200_queue_ops.  Both
+ * are plain host code (no CUDA calls). */
+typedef struct mayo_b200_serve_req {
+    const uint8_t *msg; /* mlen bytes */
+    const uint8_t *sig; /* verify: sig_bytes of the set; unused for sign */
+    uint8_t *out;       /* sign: sig_bytes of the set; verify: 1 byte */
+    uint32_t mlen;
+    uint32_t key_id;    /* the caller's key id (not read here) */
+    uint32_t key_slot;  /* row of the set's key table (esk for sign, epk for verify) */
+    uint8_t op;         /* MAYO_B200_OP_SIGN or MAYO_B200_OP_VERIFY */
+    uint8_t set;        /* 1, 2, 3, 5 */
+    uint8_t pad[2];
+} mayo_b200_serve_req;
+typedef struct mayo_b200_serve_group {
+    uint32_t count; /* 0: the group is absent */
+    uint32_t set, op, pad;
+    uint64_t key_off, len_off, msg_off, sig_off; /* input staging offsets */
+    uint64_t out_off;                            /* output staging offset */
+} mayo_b200_serve_group;
+typedef struct mayo_b200_serve_layout {
+    uint32_t n, max_msg;
+    uint64_t in_bytes, out_bytes;
+    mayo_b200_serve_group group[8]; /* group 2*(set index) + (op == VERIFY) */
+} mayo_b200_serve_layout;
+/* Bytes of input / output staging a batch of n requests needs at most. */
+MAYO_B200_API size_t mayo_b200_serve_in_bytes(uint32_t n, uint32_t max_msg);
+MAYO_B200_API size_t mayo_b200_serve_out_bytes(uint32_t n);
+/* MAYO_B200_ERR_ARG for an op other than sign / verify, an unknown set, mlen > max_msg, a NULL
+ * message with mlen > 0, a NULL signature or output, or staging smaller than the layout. */
+MAYO_B200_API int mayo_b200_serve_pack(const mayo_b200_serve_req *req, uint32_t n, uint32_t max_msg,
+                                       uint8_t *stage_in, size_t in_capacity, size_t out_capacity,
+                                       mayo_b200_serve_layout *layout);
+MAYO_B200_API int mayo_b200_serve_unpack(const mayo_b200_serve_req *req, uint32_t n,
+                                         const mayo_b200_serve_layout *layout, const uint8_t *stage_out);
 
 /* ---- Sign without caller workspace.  No counterpart in the reference API. ----
  * For callers that cannot allocate device memory (a service whose device-memory budget is

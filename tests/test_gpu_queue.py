@@ -179,8 +179,8 @@ def test_queue_operand_errors_skip_items(cuda):
     assert pb[(1, Q.OP_SIGN)]["error"] == Q.QUEUE_ERR_OPERAND  # key 4 of a 1-key table
     assert pb[(1, Q.OP_SIGN)]["finished"] == 2
     # no verify operands for MAYO_1 and none at all for MAYO_5: no kernel, the items are dropped
-    assert pb[(1, Q.OP_VERIFY)]["error"] == Q.QUEUE_ERR_OPERAND and pb[(1, Q.OP_VERIFY)]["tickets"] == 1
-    assert pb[(5, Q.OP_SIGN)]["error"] == Q.QUEUE_ERR_OPERAND and pb[(5, Q.OP_SIGN)]["tickets"] == 1
+    assert pb[(1, Q.OP_VERIFY)]["error"] == Q.QUEUE_ERR_OPERAND and pb[(1, Q.OP_VERIFY)]["taken"] == 1
+    assert pb[(5, Q.OP_SIGN)]["error"] == Q.QUEUE_ERR_OPERAND and pb[(5, Q.OP_SIGN)]["taken"] == 1
     pk = ops.kp_pk.cpu().numpy().reshape(2, z.pk_bytes)
     assert (pk == O.keypair_from_seed_batch(s, seeds)).all()
     sig = ops.sg_sig.cpu().numpy().reshape(2, z.sig_bytes)
