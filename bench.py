@@ -977,7 +977,7 @@ def run_serving(args, dist: Dist):
     # keys (all resident: 4096 keys ~ 2 GB of esk + epk, far inside the budget)
     seeds = {s: seeds_for(seed * 100 + s, SERVE_KEYS[s], M.sizes(s).sk_bytes) for s in sets}
     cache = SV.KeyCache(seeds, SV.KeyCache.capacity_for_budget(budget // 2, SERVE_KEYS), device=dev)
-    server = SV.Server(cache, max_batch=max_batch, inflight=2, max_msg=max_msg, budget_bytes=budget)
+    server = SV.Server(cache, max_batch=max_batch, inflight=args.inflight, max_msg=max_msg, budget_bytes=budget)
     for s in sets:  # load every key once, outside the timed runs
         _, su = cache.acquire(s, np.arange(SERVE_KEYS[s]), st)
         cache.release(s, su)
@@ -1122,7 +1122,7 @@ def run_serving(args, dist: Dist):
         "vs_baseline": None, "dtype": "u32 (GF(16) bit-planes)", "data": "synthetic (seeded ChaCha20)",
         "config": {"workload": "serving: open-loop Poisson arrivals, 70 % verify / 30 % sign, sets 40/30/20/10, "
                                "4096 resident keys, continuous batching over the persistent queue",
-                   "max_batch": max_batch, "inflight_batches": 2, "msg_len": f"32..{max_msg} B",
+                   "max_batch": max_batch, "inflight_batches": args.inflight, "msg_len": f"32..{max_msg} B",
                    "key_cache_bytes": cache.nbytes(), "device_bytes": server.device_bytes, "budget_bytes": budget,
                    "value": "requests/s served at an offered load of 0.8 x the closed-loop batched peak"},
         "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"], "p999_ms": head["p999_ms"],
@@ -1150,6 +1150,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--inflight", type=int, default=4, help="c5: batches on the GPU at once")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--int-peak", action="store_true",
                     help="build and run cumayo_b200/peaks/int_pipes.cu (integer-pipe rates) and exit")
