@@ -470,7 +470,10 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
             my_has[q] = found;
         }
         __syncthreads();
-        // every column: col ^= col[p] * F'  (eliminates row p elsewhere, normalises row p)
+        // every column right of pc: col ^= col[p] * F'  (eliminates row p elsewhere, normalises
+        // row p).  A column left of pc is already a unit vector e_p' (or has no entry in an
+        // unpivoted row), so col[p] = 0 there for every later pivot row p and the update would be
+        // a no-op; skipping it depends only on the public loop index.
         G4 F[W];
         uint32_t oh[W];
 #pragma unroll
@@ -480,6 +483,8 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
         }
 #pragma unroll
         for (int q = 0; q < CPT; q++) {
+            const int c = tid + NT * q;
+            if (c <= pc || c >= C::NCOL) continue;
             uint32_t e0 = 0, e1 = 0, e2 = 0, e3 = 0;
 #pragma unroll
             for (int w = 0; w < W; w++) {
