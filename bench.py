@@ -196,6 +196,8 @@ def run_ours(args, dist: Dist):
     launches_per_step = 0
     seed = 1 + dist.rank
     plain_fn = None
+    plain_api = "per-(set, op) batched launches: keypair_from_seed, sign_many, verify_many"
+    plain_check = None
 
     if wl["kind"] == "shared_sign_verify":
         # one resident expanded key (esk, epk), messages of per-instance length
@@ -218,17 +220,33 @@ def run_ours(args, dist: Dist):
         d_offs = h_offs.to(dev)
         d_lens = h_lens.to(dev)
         sig = torch.zeros(batch * z.sig_bytes, dtype=torch.uint8, device=dev)
-        ws = torch.zeros(batch * m.sign_ws_bytes(), dtype=torch.uint8, device=dev)
+        # one workspace serves both calls (verify runs after sign on the same stream)
+        ws = torch.zeros(max(m.sign_shared_ws_bytes(batch), m.verify_shared_ws_bytes(batch)), dtype=torch.uint8,
+                         device=dev)
         res = torch.zeros(batch, dtype=torch.uint8, device=dev)
         h_sig = torch.zeros(batch * z.sig_bytes, dtype=torch.uint8).pin_memory()
         h_res = torch.zeros(batch, dtype=torch.uint8).pin_memory()
-        launches_per_step = 3  # sign: hash + core; verify: one
+        launches_per_step = 7  # sign: hash, key tiles, tensor-core product, tail; verify: the last three
 
         def sign_op():
-            m.sign_many(esk, d_msgs, sig, ws, batch, msg_off=d_offs, msg_len=d_lens, stream=st)
+            m.sign_shared(esk, d_msgs, sig, ws, batch, msg_off=d_offs, msg_len=d_lens, stream=st)
 
         def verify_op():
-            m.verify_many(epk, d_msgs, sig, res, batch, msg_off=d_offs, msg_len=d_lens, stream=st)
+            m.verify_shared(epk, d_msgs, sig, res, ws, batch, msg_off=d_offs, msg_len=d_lens, stream=st)
+
+        # the per-instance engine path (sign_many / verify_many with a shared key), same work
+        ws_many = torch.zeros(batch * m.sign_ws_bytes(), dtype=torch.uint8, device=dev)
+        sig_many = torch.zeros_like(sig)
+        res_many = torch.zeros_like(res)
+
+        def plain_fn():
+            m.sign_many(esk, d_msgs, sig_many, ws_many, batch, msg_off=d_offs, msg_len=d_lens, stream=st)
+            m.verify_many(epk, d_msgs, sig_many, res_many, batch, msg_off=d_offs, msg_len=d_lens, stream=st)
+
+        plain_api = "per-instance engine: mayo_b200_sign_many / verify_many with esk/epk stride 0"
+
+        def plain_check():  # the two paths must agree byte for byte
+            return int((sig_many != sig).sum().item()) + int((res_many != res).sum().item())
 
         def h2d():
             d_msgs.copy_(h_msgs, non_blocking=True)
@@ -245,11 +263,12 @@ def run_ours(args, dist: Dist):
         ops_per_step = 2 * batch
         macs = mac_counts(s)
         work = {"sign": macs["sign"] * batch, "verify": macs["verify"] * batch}
-        hbm_bytes = {"sign": z.esk_bytes + body.nbytes + batch * (z.sig_bytes + 2 * m.sign_ws_bytes()),
+        hbm_bytes = {"sign": z.esk_bytes + body.nbytes + batch * z.sig_bytes,
                      "verify": z.epk_bytes + body.nbytes + batch * (z.sig_bytes + 1)}
         cfg = {"workload": "MAYO_2 shared-key sign+verify", "set": "MAYO_2", "batch": batch,
                "msg_len": "uniform 32..1024 B", "key": "one expanded key resident in HBM",
-               "l2": "flushed between steps (256 MiB write)", "api": "mayo_b200_sign_many / verify_many"}
+               "l2": "flushed between steps (256 MiB write)",
+               "api": "mayo_b200_sign_shared / verify_shared (key products on the tensor cores)"}
         expected = np.zeros(batch, np.uint8)
         res_dev = lambda: res  # noqa: E731
     elif wl["kind"] == "keypair_sign_verify":
@@ -484,7 +503,9 @@ def run_ours(args, dist: Dist):
         torch.cuda.synchronize()
         plain_ms = dist.max(p0.elapsed_time(p1)) / args.steps
         out["plain"] = {"value": round(ops_per_step * dist.world / (plain_ms / 1e3), 1), "ms_per_step": round(plain_ms, 4),
-                        "api": "per-(set, op) batched launches: keypair_from_seed, sign_many, verify_many"}
+                        "api": plain_api}
+        if plain_check is not None:
+            out["result_mismatches"] += plain_check()
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
     return out

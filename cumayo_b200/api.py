@@ -94,6 +94,13 @@ def lib() -> ctypes.CDLL:
         L.mayo_b200_sign_noalloc_max_batch.argtypes = [ctypes.c_int]
         L.mayo_b200_sign_many_noalloc.restype = ctypes.c_int
         L.mayo_b200_sign_many_noalloc.argtypes = [ctypes.c_int, vp, sz, vp, vp, vp, sz, sz, vp, sz, sz, vp]
+        for nm in ("sign_shared_ws_bytes", "verify_shared_ws_bytes"):
+            getattr(L, "mayo_b200_" + nm).restype = ctypes.c_size_t
+            getattr(L, "mayo_b200_" + nm).argtypes = [ctypes.c_int, sz]
+        L.mayo_b200_sign_shared.restype = ctypes.c_int
+        L.mayo_b200_sign_shared.argtypes = [ctypes.c_int, vp, vp, vp, vp, sz, sz, vp, sz, vp, sz, vp]
+        L.mayo_b200_verify_shared.restype = ctypes.c_int
+        L.mayo_b200_verify_shared.argtypes = [ctypes.c_int, vp, vp, vp, vp, sz, sz, vp, sz, vp, vp, sz, vp]
         _lib = L
     return _lib
 
@@ -291,6 +298,31 @@ class Mayo:
                                            _ptr(msg_len), msg_stride, mlen, _ptr(sig),
                                            z.sig_bytes if sig_stride is None else sig_stride, _ptr(result), batch,
                                            _stream(stream)), "verify_many")
+
+    def sign_shared_ws_bytes(self, batch: int) -> int:
+        return int(lib().mayo_b200_sign_shared_ws_bytes(self.set, batch))
+
+    def verify_shared_ws_bytes(self, batch: int) -> int:
+        return int(lib().mayo_b200_verify_shared_ws_bytes(self.set, batch))
+
+    def sign_shared(self, esk, msgs, sig, ws, batch, *, msg_off=None, msg_len=None, msg_stride=0, mlen=0,
+                    sig_stride=None, stream=None):
+        """sign_many under one expanded key for the whole batch, the key's products on the tensor
+        cores.  ws: device memory of sign_shared_ws_bytes(batch) bytes, 16-byte aligned."""
+        z = self.sizes
+        _check(lib().mayo_b200_sign_shared(self.set, _ptr(esk), _ptr(msgs), _ptr(msg_off), _ptr(msg_len), msg_stride,
+                                           mlen, _ptr(sig), z.sig_bytes if sig_stride is None else sig_stride,
+                                           _ptr(ws), batch, _stream(stream)), "sign_shared")
+
+    def verify_shared(self, epk, msgs, sig, result, ws, batch, *, msg_off=None, msg_len=None, msg_stride=0, mlen=0,
+                      sig_stride=None, stream=None):
+        """verify_many under one expanded public key for the whole batch, the key's products on
+        the tensor cores.  ws: device memory of verify_shared_ws_bytes(batch) bytes."""
+        z = self.sizes
+        _check(lib().mayo_b200_verify_shared(self.set, _ptr(epk), _ptr(msgs), _ptr(msg_off), _ptr(msg_len),
+                                             msg_stride, mlen, _ptr(sig),
+                                             z.sig_bytes if sig_stride is None else sig_stride, _ptr(result),
+                                             _ptr(ws), batch, _stream(stream)), "verify_shared")
 
     def sign_noalloc_max_batch(self) -> int:
         return int(lib().mayo_b200_sign_noalloc_max_batch(self.set))

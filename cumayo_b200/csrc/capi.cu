@@ -359,4 +359,43 @@ MAYO_B200_API int mayo_b200_verify_many(int set, const uint8_t *epk, size_t epk_
     return kernel_rc(launch_verify_io(set, io, batch, S_(stream)));
 }
 
+MAYO_B200_API size_t mayo_b200_sign_shared_ws_bytes(int set, size_t batch) {
+    return mayo::shared_ws_bytes(set, false, batch);
+}
+
+MAYO_B200_API int mayo_b200_sign_shared(int set, const uint8_t *esk, const uint8_t *msgs, const uint64_t *msg_off,
+                                        const uint32_t *msg_len, size_t msg_stride, size_t mlen, uint8_t *sig,
+                                        size_t sig_stride, uint8_t *ws, size_t batch, void *stream) {
+    Sz z;
+    if (!sizes_of(set, z)) return MAYO_B200_ERR_SET;
+    if (batch == 0) return MAYO_B200_OK;
+    if (!esk || !sig || !ws || batch > 0x7fffffffu || mlen > 0x7fffffffu) return MAYO_B200_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(ws) & 15) return MAYO_B200_ERR_ARG;  // bulk copies need 16-byte alignment
+    if ((msg_off == nullptr) != (msg_len == nullptr)) return MAYO_B200_ERR_ARG;
+    if (!msgs && (msg_off || mlen)) return MAYO_B200_ERR_ARG;
+    if (batch > 1 && sig_stride < z.sig) return MAYO_B200_ERR_ARG;
+    SignIO io{esk, 0, MsgIO{msgs, msg_stride, msg_off, msg_len, (uint32_t)mlen}, sig, sig_stride, nullptr, 0};
+    return kernel_rc(mayo::launch_sign_shared(set, io, ws, batch, S_(stream)));
+}
+
+MAYO_B200_API size_t mayo_b200_verify_shared_ws_bytes(int set, size_t batch) {
+    return mayo::shared_ws_bytes(set, true, batch);
+}
+
+MAYO_B200_API int mayo_b200_verify_shared(int set, const uint8_t *epk, const uint8_t *msgs, const uint64_t *msg_off,
+                                          const uint32_t *msg_len, size_t msg_stride, size_t mlen, const uint8_t *sig,
+                                          size_t sig_stride, uint8_t *result, uint8_t *ws, size_t batch,
+                                          void *stream) {
+    Sz z;
+    if (!sizes_of(set, z)) return MAYO_B200_ERR_SET;
+    if (batch == 0) return MAYO_B200_OK;
+    if (!epk || !sig || !result || !ws || batch > 0x7fffffffu || mlen > 0x7fffffffu) return MAYO_B200_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(ws) & 15) return MAYO_B200_ERR_ARG;
+    if ((msg_off == nullptr) != (msg_len == nullptr)) return MAYO_B200_ERR_ARG;
+    if (!msgs && (msg_off || mlen)) return MAYO_B200_ERR_ARG;
+    if (batch > 1 && sig_stride < z.sig) return MAYO_B200_ERR_ARG;
+    VerifyIO io{epk, 0, MsgIO{msgs, msg_stride, msg_off, msg_len, (uint32_t)mlen}, sig, sig_stride, result, 1};
+    return kernel_rc(mayo::launch_verify_shared(set, io, ws, batch, S_(stream)));
+}
+
 }  // extern "C"

@@ -1,0 +1,557 @@
+// op_shared.cu -- sign / verify of a batch under ONE key, with the key's heavy products on the
+// tensor cores (tcgen05.mma, kind::i8).
+//
+// The per-instance engine (engine.cuh) spends most of a signature on T_j[r] = sum_c P1[r][c] V_j[c]
+// (U = V^T P1 V) and M_j[b] = sum_a V_j[a] L[a][b] (src/sign.cu:254-330, 396-437), and most of a
+// verification on T_j[r] = sum_c P[r][c] s_j[c] (src/verify.cu:72-182).  When every instance of a
+// batch uses the same key these are one matrix product over the whole batch: GF(16) is GF(2)^4,
+// multiplication by a field element a is the 4x4 bit matrix Mul(a)[b][b'] = bit b of (a * x^b'),
+// so with every entry expanded to its bit matrix
+//     bit b of coordinate t of T_j[r]  =  sum over (c, b') of  Mul(P[r][c]_t)[b][b'] * bit b' of V_j[c]   (mod 2)
+// -- a 0/1 matrix A (rows (r, t, b), columns (c, b')) times a 0/1 matrix B (rows (c, b'),
+// columns (instance, j)).  The tensor cores sum the products exactly in s32 and the epilogue
+// keeps bit 0 of each sum.
+//
+// Kernels:
+//   shared_a_kernel     builds A from the key, tiled for the MMA (one 128-row tile = the four bit
+//                       planes of one 32-coordinate group of one row r) in the K-major, no-swizzle
+//                       shared-memory layout, so a tile moves to shared memory with one bulk copy.
+//   shared_gemm_kernel  one CTA per N instances' vectors (B, built in shared memory from their
+//                       nibbles, resident): for every A tile, a bulk copy (double-buffered), one
+//                       thread issues the MMAs into a TMEM accumulator (double-buffered), and eight
+//                       warps read the accumulator back (tcgen05.ld), take bit 0 of each sum with
+//                       warp ballots -- one ballot is one 32-coordinate bit plane -- and store the
+//                       planes.  Zero blocks of A (columns c < r of the triangular P1 / P) are
+//                       skipped.  Waits are bounded: a timeout sets the status word and unwinds.
+//   sign: sign_hash_kernel (thread per instance) -> product -> sign_shared_tail_kernel (first
+//         attempt from the planes in a compact CTA) -> sign_shared_fix_kernel (retries of the
+//         rare singular first attempts with the engine).
+//   verify: verify_hash_kernel (thread per instance: digest, t) -> product ->
+//         verify_shared_tail_kernel (U from the planes, Horner, compare; a small CTA).
+//   If the status word shows a failed product, the tails do nothing and the fix-up kernels run
+//   every instance through the per-instance engine, so results stay correct.
+#include <cuda_runtime.h>
+
+#include "../../include/mayo_b200.h"
+#include "launch_util.cuh"
+#include "ops.h"
+#include "sign_body.cuh"
+#include "tc.cuh"
+#include "verify_body.cuh"
+
+namespace mayo {
+
+constexpr uint32_t SH_SPIN = 1u << 22;  // mbarrier polls before a wait gives up
+constexpr size_t SH_SMEM_MAX = 220 * 1024;
+constexpr int SH_GEMM_NT = 256;  // 8 warps: warp w reads TMEM lanes 32 (w % 4).., columns half w / 4
+constexpr int SH_FIX_CTAS = 2 * 148;
+
+// The product for sign (rows: T_j[r] over P1 for r < v, then M_j[b] over L) or verify (rows
+// T_j[r] over [[P1, P2], [0, P3]] for r < n).
+template <int SET, bool VERIFY>
+struct SharedProb {
+    using S = Set<SET>;
+    static constexpr int W = S::W;
+    static constexpr int NVEC = VERIFY ? S::n : S::v;         // entries of one vector V_j / s_j
+    static constexpr int NROWS = VERIFY ? S::n : S::v + S::o;  // m-vector rows of the result
+    static constexpr int KPAD = (4 * NVEC + 31) / 32 * 32;    // bytes of one B column (K)
+    static constexpr int KSTEPS = KPAD / 32;                   // MMAs of K = 32 per tile
+    static constexpr int NTILES = NROWS * W;
+    static constexpr size_t TILE = (size_t)128 * KPAD;
+    static constexpr size_t smem_for(int N) { return (size_t)N * KPAD + 2 * TILE + (size_t)N * 16 + 64; }
+    static constexpr int N = smem_for(256) <= SH_SMEM_MAX ? 256 : (smem_for(128) <= SH_SMEM_MAX ? 128 : 64);
+    static constexpr int NI = N / S::k;  // instances per CTA
+    static constexpr size_t SMEM = smem_for(N);
+    static constexpr size_t PLANES = (size_t)S::k * NROWS * W;  // uint4 per instance
+    // first column c that can be nonzero in row rr
+    __host__ __device__ static constexpr int c_min(int rr) { return VERIFY ? rr : (rr < S::v ? rr : 0); }
+    // coordinate t of entry (rr, c) of the key matrix, 0 where it is structurally zero
+    __device__ static uint32_t entry(const uint8_t *key, int rr, int c, int t) {
+        const uint8_t *e = nullptr;
+        if (VERIFY) {  // key = epk = P1 || P2 || P3
+            if (c >= rr) {
+                if (rr < S::v)
+                    e = c < S::v ? key + (size_t)tri(rr, c, S::v) * S::menc
+                                 : key + S::p1 + (size_t)(rr * S::o + (c - S::v)) * S::menc;
+                else
+                    e = key + S::p1 + S::p2 + (size_t)tri(rr - S::v, c - S::v, S::o) * S::menc;
+            }
+        } else {  // key = esk = seed_sk || O || P1 || L
+            const uint8_t *P1 = key + S::sk + S::o_bytes, *L = P1 + S::p1;
+            if (rr < S::v) {
+                if (c >= rr) e = P1 + (size_t)tri(rr, c, S::v) * S::menc;
+            } else {
+                e = L + (size_t)(c * S::o + (rr - S::v)) * S::menc;
+            }
+        }
+        return e ? (e[t >> 1] >> ((t & 1) * 4)) & 0xFu : 0u;
+    }
+};
+
+// Workspace: control words ([0] status: 0 = product ran, 1 = it gave up; [1] sign retries), A
+// tiles, per-instance hash results (sign: digest, salt, t, V || r; verify: t), per-instance
+// planes, (sign) the list of instances whose first attempt was singular.
+template <int SET, bool VERIFY>
+struct SharedWs {
+    using P = SharedProb<SET, VERIFY>;
+    static constexpr int NW = (Set<SET>::menc + 3) / 4;
+    static constexpr size_t a = 256;
+    static constexpr size_t a_bytes = (size_t)P::NTILES * P::TILE;
+    static constexpr size_t inst = VERIFY ? pad16((size_t)NW * 4) : pad16(SignWs<SET>::total);
+    static constexpr size_t planes = P::PLANES * 16;
+    static constexpr size_t retry = VERIFY ? 0 : 4;
+    static size_t bytes(size_t batch) { return a + a_bytes + batch * (inst + planes + retry); }
+    static size_t inst_off() { return a + a_bytes; }
+    static size_t planes_off(size_t batch) { return a + a_bytes + batch * inst; }
+    static size_t retry_off(size_t batch) { return a + a_bytes + batch * (inst + planes); }
+};
+
+// A, tiled: tile tt = rr * W + w holds rows rho = 32 b + t' (bit plane b, lane t'; lane t' carries
+// coordinate 32 w + 8 (t' & 3) + (t' >> 2), the bit order of a G4 plane) and K bytes 4 c + b';
+// layout [K / 16][128 rows][16 bytes].  One thread per 16 bytes.  Also resets the control words.
+template <int SET, bool VERIFY>
+__global__ void shared_a_kernel(const uint8_t *key, uint8_t *A, uint32_t *ctl) {
+    using P = SharedProb<SET, VERIFY>;
+    using S = Set<SET>;
+    constexpr size_t per_tile = (size_t)(P::KPAD / 16) * 128;
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < 2) ctl[idx] = 0;
+    if (idx >= (size_t)P::NTILES * per_tile) return;
+    const int tt = (int)(idx / per_tile);
+    const int rem = (int)(idx - (size_t)tt * per_tile);
+    const int ch = rem / 128, rho = rem - ch * 128;
+    const int rr = tt / P::W, w = tt - rr * P::W, b = rho >> 5, tp = rho & 31;
+    const int t = 32 * w + 8 * (tp & 3) + (tp >> 2);
+    uint32_t wd[4] = {0u, 0u, 0u, 0u};
+    if (t < S::m) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int c = 4 * ch + q;
+            if (c >= P::NVEC) continue;
+            const uint32_t a = P::entry(key, rr, c, t);
+            uint32_t v = 0;
+#pragma unroll
+            for (int bp = 0; bp < 4; bp++) v |= ((gf16_mul_ct(a, 1u << bp) >> b) & 1u) << (8 * bp);
+            wd[q] = v;
+        }
+    }
+    *reinterpret_cast<uint4 *>(A + (size_t)tt * P::TILE + (size_t)ch * 2048 + (size_t)rho * 16) =
+        make_uint4(wd[0], wd[1], wd[2], wd[3]);
+}
+
+// vec: instance i's vectors start at vec + i * vec_stride, entry c of vector j is nibble
+// j * NVEC + c.  planes: instance i at planes + i * PLANES, [j][row][w].
+template <int SET, bool VERIFY>
+__global__ void __launch_bounds__(SH_GEMM_NT, 1)
+    shared_gemm_kernel(const uint8_t *__restrict__ A, const uint8_t *__restrict__ vec, size_t vec_stride,
+                       uint4 *__restrict__ planes, uint32_t batch, uint32_t *ctl) {
+    using P = SharedProb<SET, VERIFY>;
+    using S = Set<SET>;
+    constexpr int N = P::N, KPAD = P::KPAD, NT = P::NTILES, W = P::W;
+    constexpr uint32_t TILE = (uint32_t)P::TILE;
+    constexpr uint32_t IDESC = tc::idesc_u8(128, N);
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *sB = smem;                                            // [KPAD/16][N][16]
+    uint8_t *sA = smem + (size_t)N * KPAD;                          // 2 x [KPAD/16][128][16]
+    uint32_t *sTB = reinterpret_cast<uint32_t *>(sA + 2 * (size_t)TILE);  // [N][4] planes of one tile
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sTB + 4 * N);    // full[2], mma_done[2]
+    uint32_t *s_tmem = reinterpret_cast<uint32_t *>(bars + 4);
+    uint32_t *s_fail = s_tmem + 1;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int plane = warp & 3, half = warp >> 2;
+    const uint32_t inst0 = blockIdx.x * (uint32_t)P::NI;
+
+    if (tid == 0) {
+        for (int i = 0; i < 4; i++) tc::mbar_init(&bars[i], 1);
+        tc::fence_mbar_init();
+        *s_fail = 0;
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(s_tmem, 2 * N);
+        tc::tmem_relinquish();
+    }
+    // B: column n = (instance n / k, vector j = n % k); K byte 4 c + b' = bit b' of entry c
+    for (int idx = tid; idx < (KPAD / 16) * N; idx += SH_GEMM_NT) {
+        const int ch = idx / N, n = idx - ch * N;
+        const uint32_t inst = inst0 + (uint32_t)(n / S::k);
+        const int j = n % S::k;
+        uint32_t wd[4] = {0u, 0u, 0u, 0u};
+        if (n < P::NI * S::k && inst < batch) {
+            const uint8_t *vp = vec + (size_t)inst * vec_stride;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int c = 4 * ch + q;
+                if (c < P::NVEC) {
+                    const int nib = j * P::NVEC + c;
+                    const uint32_t x = (vp[nib >> 1] >> ((nib & 1) * 4)) & 0xFu;
+                    wd[q] = (x * 0x00204081u) & 0x01010101u;  // bit b' -> byte b'
+                }
+            }
+        }
+        *reinterpret_cast<uint4 *>(sB + ((size_t)ch * N + n) * 16) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+    }
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = *s_tmem;
+    const uint32_t sA_addr = tc::smem_u32(sA), sB_addr = tc::smem_u32(sB);
+
+    // thread 0's bookkeeping of asynchronous work, for the unwind after a timeout
+    uint32_t ld_issued[2] = {0u, 0u}, ld_waited[2] = {0u, 0u}, mma_issued[2] = {0u, 0u}, mma_waited[2] = {0u, 0u};
+    auto load = [&](int tile) {
+        const int b = tile & 1;
+        tc::mbar_arrive_expect_tx(&bars[b], TILE);
+        tc::bulk_g2s(sA + (size_t)b * TILE, A + (size_t)tile * TILE, TILE, &bars[b]);
+        ld_issued[b]++;
+    };
+    auto issue = [&](int tile) -> bool {
+        const int b = tile & 1;
+        if (!tc::mbar_wait(&bars[b], ld_waited[b] & 1u, SH_SPIN)) return false;
+        ld_waited[b]++;
+        tc::fence_after_sync();
+        const int s0 = P::c_min(tile / W) / 8;  // K bytes 32 s .. 32 s + 31 hold columns 8 s .. 8 s + 7
+        for (int s = s0; s < P::KSTEPS; s++) {
+            const uint64_t ad = tc::desc_kmajor(sA_addr + (uint32_t)b * TILE + (uint32_t)s * 4096u, 2048u, 128u);
+            const uint64_t bd = tc::desc_kmajor(sB_addr + (uint32_t)s * 2u * N * 16u, (uint32_t)N * 16u, 128u);
+            tc::mma_i8(tbase + (uint32_t)b * N, ad, bd, IDESC, s > s0 ? 1u : 0u);
+        }
+        tc::mma_commit(&bars[2 + b]);
+        mma_issued[b]++;
+        return true;
+    };
+
+    if (tid == 0) {
+        load(0);
+        if (NT > 1) load(1);
+        if (!issue(0)) *s_fail = 1;
+    }
+    __syncthreads();
+    const uint32_t lane_base = (uint32_t)(plane * 32) << 16;
+#pragma unroll 1
+    for (int i = 0; i < NT && !*s_fail; i++) {
+        const int b = i & 1;
+        if (tid == 0 && i + 1 < NT && !issue(i + 1)) atomicOr(s_fail, 1u);
+        // the MMAs of tile i
+        const bool done = tc::mbar_wait(&bars[2 + b], (uint32_t)(i >> 1) & 1u, SH_SPIN);
+        if (!done) atomicOr(s_fail, 1u);
+        if (tid == 0 && done) mma_waited[b]++;
+        tc::fence_after_sync();
+        // its A buffer is free: prefetch tile i + 2
+        if (tid == 0 && done && i + 2 < NT) load(i + 2);
+        // epilogue: bit 0 of each sum; warp (plane, half) reads plane `plane` (TMEM lanes
+        // 32 plane..) of columns [half N/2, (half + 1) N/2); one ballot = one 32-coordinate word
+#pragma unroll 1
+        for (int ch = 0; ch < N / 64; ch++) {
+            const int col0 = half * (N / 2) + ch * 32;
+            uint32_t r[32];
+            tc::tmem_ld32(tbase + lane_base + (uint32_t)(b * N + col0), r);
+            tc::tmem_wait_ld();
+            uint32_t mine = 0;
+#pragma unroll
+            for (int q = 0; q < 32; q++) {
+                const uint32_t word = __ballot_sync(0xffffffffu, r[q] & 1u);
+                if (lane == q) mine = word;
+            }
+            sTB[(col0 + lane) * 4 + plane] = mine;
+        }
+        tc::fence_before_sync();
+        __syncthreads();
+        const int rr = i / W, w = i - rr * W;
+        for (int n = tid; n < P::NI * S::k; n += SH_GEMM_NT) {
+            const uint32_t inst = inst0 + (uint32_t)(n / S::k);
+            const int j = n % S::k;
+            if (inst < batch)
+                planes[(size_t)inst * P::PLANES + ((size_t)j * P::NROWS + rr) * W + w] =
+                    *reinterpret_cast<const uint4 *>(sTB + 4 * n);
+        }
+        __syncthreads();
+    }
+    // unwind: no bulk copy or MMA of this CTA may still be in flight when TMEM is freed
+    if (tid == 0) {
+        for (int b = 0; b < 2; b++) {
+            while (ld_waited[b] < ld_issued[b] && tc::mbar_wait(&bars[b], ld_waited[b] & 1u, SH_SPIN)) ld_waited[b]++;
+            while (mma_waited[b] < mma_issued[b] &&
+                   tc::mbar_wait(&bars[2 + b], mma_waited[b] & 1u, SH_SPIN))
+                mma_waited[b]++;
+        }
+        if (*s_fail) atomicOr(ctl, 1u);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tbase, 2 * N);
+    }
+}
+
+// ---- sign ----
+// First attempt from the planes, in a CTA without engine staging (more CTAs per SM).  A singular
+// first attempt goes to the retry list; the fix-up kernel finishes it with the engine.
+template <int SET>
+__global__ void __launch_bounds__(SignCfg<SET>::NT)
+    sign_shared_tail_kernel(const uint8_t *esk, uint8_t *sig, size_t sig_stride, const uint8_t *wsi, size_t wsi_stride,
+                            const uint4 *planes, uint32_t *ctl, uint32_t *retry) {
+    using P = SharedProb<SET, false>;
+    extern __shared__ __align__(16) uint8_t smem[];
+    constexpr int NT = SignCfg<SET>::NT;
+    if (ctl[0]) return;  // the product gave up: the fix-up kernel signs everything
+    const int tid = threadIdx.x;
+    const uint32_t inst = blockIdx.x;
+    sign_load_ws<SET, NT, true>(smem, tid, esk, wsi + (size_t)inst * wsi_stride);
+    if (sign_attempt<SET, NT, true>(smem, tid, esk, planes + (size_t)inst * P::PLANES)) {
+        sign_write<SET, NT, true>(smem, tid, esk, sig + (size_t)inst * sig_stride);
+    } else if (tid == 0) {
+        retry[atomicAdd(&ctl[1], 1u)] = inst;
+    }
+}
+
+// Retries (attempts ctr >= 1 of the listed instances) with the engine, or every instance from
+// ctr = 0 if the product gave up.  A grid-stride loop over a count read on the device.
+template <int SET>
+__global__ void __launch_bounds__(SignCfg<SET>::NT)
+    sign_shared_fix_kernel(const uint8_t *esk, uint8_t *sig, size_t sig_stride, const uint8_t *wsi, size_t wsi_stride,
+                           const uint32_t *ctl, const uint32_t *retry, uint32_t batch) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    constexpr int NT = SignCfg<SET>::NT;
+    const int tid = threadIdx.x;
+    const bool all = ctl[0] != 0;
+    const uint32_t count = all ? batch : ctl[1];
+#pragma unroll 1
+    for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
+        const uint32_t inst = all ? idx : retry[idx];
+        sign_load_ws<SET, NT>(smem, tid, esk, wsi + (size_t)inst * wsi_stride);
+#pragma unroll 1
+        for (int ctr = all ? 0 : 1; ctr < 255; ctr++) {
+            if (ctr > 0) sign_next_vr<SET, NT>(smem, tid, ctr);
+            if (sign_attempt<SET, NT>(smem, tid, esk)) break;
+        }
+        sign_write<SET, NT>(smem, tid, esk, sig + (size_t)inst * sig_stride);
+        __syncthreads();
+    }
+}
+
+// ---- verify ----
+// Thread per instance: digest = SHAKE256(M), t = SHAKE256(digest || salt) (src/verify.cu:37-48).
+template <int SET>
+__global__ void verify_hash_kernel(const VerifyIO io, uint8_t *tws, size_t tws_stride, uint32_t batch) {
+    using S = Set<SET>;
+    const uint32_t inst = blockIdx.x * blockDim.x + threadIdx.x;
+    if (inst >= batch) return;
+    uint8_t digest[S::digest];
+    Sponge<136> sp;
+    sp.init();
+    sp.absorb(io.m.ptr(inst), io.m.len(inst));
+    sp.finalize();
+    sp.squeeze(digest, S::digest);
+    Sponge<136> sp2;
+    sp2.init();
+    sp2.absorb(digest, S::digest);
+    sp2.absorb(io.sig + (size_t)inst * io.sig_stride + S::k * S::n / 2, S::sk);  // salt
+    sp2.finalize();
+    uint8_t *t = tws + (size_t)inst * tws_stride;
+    sp2.squeeze(t, S::menc);
+    for (int i = S::menc; i < (S::menc + 3) / 4 * 4; i++) t[i] = 0;
+}
+
+// U_ij = s_i^T T_j from the planes, y = Horner over the pairs, compare with t.  No engine
+// staging, no hashing: a small CTA.
+template <int SET>
+struct VTailCfg {
+    using S = Set<SET>;
+    static constexpr int J = S::k, W = S::W, NW = (S::menc + 3) / 4, NT = 128;
+    static constexpr int R = NT / (J * W);
+    static_assert(R >= 1, "verify tail threads");
+    static constexpr size_t off_masks = 0;
+    static constexpr size_t off_x = off_masks + (size_t)S::n * J * 16;
+    static constexpr size_t off_upk = off_x + (size_t)J * J * W * 16;
+    static constexpr size_t off_t = off_upk + pad16((size_t)S::pairs * NW * 4);
+    static constexpr size_t total = off_t + pad16((size_t)NW * 4);
+};
+
+template <int SET>
+__global__ void __launch_bounds__(VTailCfg<SET>::NT)
+    verify_shared_tail_kernel(const VerifyIO io, const uint8_t *tws, size_t tws_stride, const uint4 *planes,
+                              const uint32_t *ctl) {
+    using S = Set<SET>;
+    using C = VTailCfg<SET>;
+    using P = SharedProb<SET, true>;
+    constexpr int J = C::J, W = C::W, NW = C::NW, R = C::R;
+    extern __shared__ __align__(16) uint8_t smem[];
+    if (ctl[0]) return;  // the product gave up: the fix-up kernel verifies everything
+    uint4 *masks = reinterpret_cast<uint4 *>(smem + C::off_masks);
+    uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
+    uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
+    uint32_t *s_t = reinterpret_cast<uint32_t *>(smem + C::off_t);
+    const int tid = threadIdx.x;
+    const size_t inst = blockIdx.x;
+    const uint8_t *sig = io.sig + inst * io.sig_stride;
+    for (int idx = tid; idx < S::n * J; idx += C::NT) {  // column c of s_j (src/verify.cu:62-70)
+        const int c = idx / J, jj = idx - c * J;
+        const int q = jj * S::n + c;
+        masks[idx] = scalar_masks((sig[q >> 1] >> ((q & 1) * 4)) & 0xFu);
+    }
+    for (int i = tid; i < J * J * W * 4; i += C::NT) reinterpret_cast<uint32_t *>(xacc)[i] = 0;
+    for (int i = tid; i < NW; i += C::NT) s_t[i] = reinterpret_cast<const uint32_t *>(tws + inst * tws_stride)[i];
+    __syncthreads();
+    if (tid < J * W * R) {
+        const int j = tid % J, w = (tid / J) % W, rs = tid / (J * W);
+        const uint4 *pl = planes + inst * P::PLANES + (size_t)j * S::n * W + w;
+        G4 X[J];
+#pragma unroll
+        for (int i = 0; i < J; i++) X[i] = g4_zero();
+#pragma unroll 1
+        for (int r = rs; r < S::n; r += R) {
+            const G4 T = g4_ld(pl + (size_t)r * W);
+            const uint4 *mr = masks + (size_t)r * J;
+#pragma unroll
+            for (int i = 0; i < J; i++) g4_madd(X[i], T, mr[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < J; i++) g4_atomic_xor(xacc + ((size_t)i * J + j) * W + w, X[i]);
+    }
+    __syncthreads();
+    for (int idx = tid; idx < S::pairs * W; idx += C::NT) {  // U_ij (i <= j) to packed words
+        const int pid = idx / W, ww = idx - pid * W;
+        int i = 0, rem = pid;
+        while (rem >= J - i) {
+            rem -= J - i;
+            i++;
+        }
+        const int j = i + rem;
+        G4 u = g4_ld(xacc + ((size_t)i * J + j) * W + ww);
+        if (i != j) u = g4_xor(u, g4_ld(xacc + ((size_t)j * J + i) * W + ww));
+        const uint4 pk = g4_to_packed(u);
+        const uint32_t wd[4] = {pk.x, pk.y, pk.z, pk.w};
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if (4 * ww + q < NW) upk[pid * NW + 4 * ww + q] = wd[q];
+    }
+    __syncthreads();
+    if (tid < 32) {  // y = Horner over the pairs (i = k-1..0, j = i..k-1), compare (src/verify.cu:185-211)
+        const int lane = tid;
+        uint32_t y = 0;
+#pragma unroll 1
+        for (int i = S::k - 1; i >= 0; i--)
+#pragma unroll 1
+            for (int j = i; j < S::k; j++) {
+                y = times_z_lane<SET>(y, lane);
+                if (lane < NW) y ^= upk[pair_index(i, j, S::k) * NW + lane];
+            }
+        const uint32_t tw = lane < NW ? s_t[lane] : 0u;
+        const bool eq = __all_sync(0xffffffffu, y == tw);
+        if (lane == 0) io.res[inst * io.res_stride] = eq ? 0 : 1;
+    }
+}
+
+// Every instance with the engine, only if the product gave up.
+template <int SET>
+__global__ void __launch_bounds__(VerifyCfg<SET>::NT)
+    verify_shared_fix_kernel(const VerifyIO io, const uint32_t *ctl, uint32_t batch) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    if (!ctl[0]) return;
+#pragma unroll 1
+    for (uint32_t inst = blockIdx.x; inst < batch; inst += gridDim.x) {
+        verify_instance<SET, VerifyCfg<SET>::NC>(smem, threadIdx.x, io.epk, io.m.ptr(inst), io.m.len(inst),
+                                                 io.sig + (size_t)inst * io.sig_stride, io.res + inst * io.res_stride);
+        __syncthreads();
+    }
+}
+
+// ---- launchers ----
+template <int SET, bool VERIFY>
+static int launch_product(const uint8_t *key, const uint8_t *vec, size_t vec_stride, uint8_t *ws, size_t batch,
+                          cudaStream_t st) {
+    using P = SharedProb<SET, VERIFY>;
+    using WSL = SharedWs<SET, VERIFY>;
+    uint32_t *ctl = reinterpret_cast<uint32_t *>(ws);
+    uint8_t *A = ws + WSL::a;
+    const size_t a_threads = (size_t)P::NTILES * (P::KPAD / 16) * 128;
+    shared_a_kernel<SET, VERIFY><<<(unsigned)((a_threads + 255) / 256), 256, 0, st>>>(key, A, ctl);
+    if (!set_smem_attr(shared_gemm_kernel<SET, VERIFY>, P::SMEM)) return ST_CUDA;
+    uint4 *planes = reinterpret_cast<uint4 *>(ws + WSL::planes_off(batch));
+    shared_gemm_kernel<SET, VERIFY><<<(unsigned)((batch + P::NI - 1) / P::NI), SH_GEMM_NT, P::SMEM, st>>>(
+        A, vec, vec_stride, planes, (uint32_t)batch, ctl);
+    return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+static unsigned fix_grid(size_t batch) { return (unsigned)(batch < SH_FIX_CTAS ? batch : SH_FIX_CTAS); }
+
+template <int SET>
+static int sign_shared_t(const SignIO &io0, uint8_t *ws, size_t batch, cudaStream_t st) {
+    using WSL = SharedWs<SET, false>;
+    using CT = SignCfg<SET, 0, true>;
+    using CF = SignCfg<SET>;
+    SignIO io = io0;
+    io.esk_stride = 0;
+    io.ws = ws + WSL::inst_off();
+    io.ws_stride = WSL::inst;
+    int rc = launch_sign_hash(SET, io, batch, st);
+    if (rc != ST_OK) return rc;
+    rc = launch_product<SET, false>(io.esk, io.ws + SignWs<SET>::vr, io.ws_stride, ws, batch, st);
+    if (rc != ST_OK) return rc;
+    uint32_t *ctl = reinterpret_cast<uint32_t *>(ws);
+    uint32_t *retry = reinterpret_cast<uint32_t *>(ws + WSL::retry_off(batch));
+    if (!set_smem_attr(sign_shared_tail_kernel<SET>, CT::total)) return ST_CUDA;
+    sign_shared_tail_kernel<SET><<<(unsigned)batch, CT::NT, CT::total, st>>>(
+        io.esk, io.sig, io.sig_stride, io.ws, io.ws_stride, reinterpret_cast<const uint4 *>(ws + WSL::planes_off(batch)),
+        ctl, retry);
+    if (!set_smem_attr(sign_shared_fix_kernel<SET>, CF::total)) return ST_CUDA;
+    sign_shared_fix_kernel<SET><<<fix_grid(batch), CF::NT, CF::total, st>>>(io.esk, io.sig, io.sig_stride, io.ws,
+                                                                            io.ws_stride, ctl, retry, (uint32_t)batch);
+    return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+template <int SET>
+static int verify_shared_t(const VerifyIO &io0, uint8_t *ws, size_t batch, cudaStream_t st) {
+    using WSL = SharedWs<SET, true>;
+    using CT = VTailCfg<SET>;
+    using CF = VerifyCfg<SET>;
+    VerifyIO io = io0;
+    io.epk_stride = 0;
+    uint8_t *tws = ws + WSL::inst_off();
+    verify_hash_kernel<SET><<<(unsigned)((batch + 127) / 128), 128, 0, st>>>(io, tws, WSL::inst, (uint32_t)batch);
+    int rc = launch_product<SET, true>(io.epk, io.sig, io.sig_stride, ws, batch, st);
+    if (rc != ST_OK) return rc;
+    const uint32_t *ctl = reinterpret_cast<const uint32_t *>(ws);
+    if (!set_smem_attr(verify_shared_tail_kernel<SET>, CT::total)) return ST_CUDA;
+    verify_shared_tail_kernel<SET><<<(unsigned)batch, CT::NT, CT::total, st>>>(
+        io, tws, WSL::inst, reinterpret_cast<const uint4 *>(ws + WSL::planes_off(batch)), ctl);
+    if (!set_smem_attr(verify_shared_fix_kernel<SET>, CF::total)) return ST_CUDA;
+    verify_shared_fix_kernel<SET><<<fix_grid(batch), CF::NT, CF::total, st>>>(io, ctl, (uint32_t)batch);
+    return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+size_t shared_ws_bytes(int set, bool verify, size_t batch) {
+    switch (set) {
+        case 1: return verify ? SharedWs<1, true>::bytes(batch) : SharedWs<1, false>::bytes(batch);
+        case 2: return verify ? SharedWs<2, true>::bytes(batch) : SharedWs<2, false>::bytes(batch);
+        case 3: return verify ? SharedWs<3, true>::bytes(batch) : SharedWs<3, false>::bytes(batch);
+        case 5: return verify ? SharedWs<5, true>::bytes(batch) : SharedWs<5, false>::bytes(batch);
+        default: return 0;
+    }
+}
+
+int launch_sign_shared(int set, const SignIO &io, uint8_t *ws, size_t batch, cudaStream_t st) {
+    if (batch == 0) return ST_OK;
+    switch (set) {
+        case 1: return sign_shared_t<1>(io, ws, batch, st);
+        case 2: return sign_shared_t<2>(io, ws, batch, st);
+        case 3: return sign_shared_t<3>(io, ws, batch, st);
+        case 5: return sign_shared_t<5>(io, ws, batch, st);
+        default: return ST_BAD_SET;
+    }
+}
+
+int launch_verify_shared(int set, const VerifyIO &io, uint8_t *ws, size_t batch, cudaStream_t st) {
+    if (batch == 0) return ST_OK;
+    switch (set) {
+        case 1: return verify_shared_t<1>(io, ws, batch, st);
+        case 2: return verify_shared_t<2>(io, ws, batch, st);
+        case 3: return verify_shared_t<3>(io, ws, batch, st);
+        case 5: return verify_shared_t<5>(io, ws, batch, st);
+        default: return ST_BAD_SET;
+    }
+}
+
+}  // namespace mayo

@@ -80,6 +80,19 @@ static int sign_t(const SignIO &io, size_t batch, cudaStream_t st) {
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
 }
 
+int launch_sign_hash(int set, const SignIO &io, size_t batch, cudaStream_t st) {
+    if (batch == 0) return ST_OK;
+    const unsigned g = (unsigned)((batch + 127) / 128);
+    switch (set) {
+        case 1: sign_hash_kernel<1><<<g, 128, 0, st>>>(io, (uint32_t)batch); break;
+        case 2: sign_hash_kernel<2><<<g, 128, 0, st>>>(io, (uint32_t)batch); break;
+        case 3: sign_hash_kernel<3><<<g, 128, 0, st>>>(io, (uint32_t)batch); break;
+        case 5: sign_hash_kernel<5><<<g, 128, 0, st>>>(io, (uint32_t)batch); break;
+        default: return ST_BAD_SET;
+    }
+    return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
 int launch_sign_io(int set, const SignIO &io, size_t batch, cudaStream_t st) {
     if (batch == 0) return ST_OK;
     switch (set) {

@@ -67,8 +67,14 @@ struct VerifyIO {
     size_t res_stride;
 };
 int launch_sign_io(int set, const SignIO &io, size_t batch, cudaStream_t st);
+// Only the hash stage of sign (digest, salt, t, V || r for ctr 0 into io.ws).
+int launch_sign_hash(int set, const SignIO &io, size_t batch, cudaStream_t st);
 int launch_verify_io(int set, const VerifyIO &io, size_t batch, cudaStream_t st);
 // Workspace bytes per instance used by sign (digest, salt, t, V || r).
 size_t sign_ws_bytes(int set);
+// One key for the whole batch, its products on the tensor cores (op_shared.cu).
+size_t shared_ws_bytes(int set, bool verify, size_t batch);
+int launch_sign_shared(int set, const SignIO &io, uint8_t *ws, size_t batch, cudaStream_t st);
+int launch_verify_shared(int set, const VerifyIO &io, uint8_t *ws, size_t batch, cudaStream_t st);
 
 }  // namespace mayo

@@ -30,7 +30,9 @@ struct SignWs {
     static_assert(total <= S::scratch, "workspace fits the reference scratch region");
 };
 
-template <int SET, int NT_ = 0>
+// COMPACT: no engine staging (the first attempt from precomputed products only); the bit-plane
+// columns of A then get a region of their own.
+template <int SET, int NT_ = 0, bool COMPACT = false>
 struct SignCfg {
     using S = Set<SET>;
     static constexpr int J = S::k, W = S::W;
@@ -43,7 +45,7 @@ struct SignCfg {
     // shared memory (bytes); the bit-plane columns of A reuse the engine staging area
     static constexpr size_t off_masks = 0;
     static constexpr size_t off_bs = off_masks + (size_t)S::v * J * 16;
-    static constexpr size_t sz_bs = (size_t)R * S::n * W * 16;
+    static constexpr size_t sz_bs = COMPACT ? 0 : (size_t)R * S::n * W * 16;
     static constexpr size_t sz_acol = (size_t)NCOL * W * 16;
     static constexpr size_t off_x = off_bs + (sz_bs > sz_acol ? sz_bs : sz_acol);
     static constexpr size_t off_upk = off_x + (size_t)J * J * W * 16;
@@ -115,12 +117,12 @@ __device__ __forceinline__ uint32_t zdown_word(const uint32_t *u, int q, int shi
 // Shared-memory views of one signing CTA.
 #define MAYO_SIGN_VIEWS                                                                       \
     using S = Set<SET>;                                                                       \
-    using C = SignCfg<SET, NT_>;                                                              \
+    using C = SignCfg<SET, NT_, CP_>;                                                         \
     constexpr int J = C::J, W = C::W, R = C::R, NT = C::NT, NW = C::NW, KO = S::ko, CPT = C::CPT; \
     (void)J; (void)R; (void)KO; (void)CPT; (void)NW;
 
 // Plain path: digest, salt, t and V||r(ctr = 0) from the workspace written by sign_hash_kernel.
-template <int SET, int NT_>
+template <int SET, int NT_, bool CP_ = false>
 __device__ __forceinline__ void sign_load_ws(uint8_t *smem, int tid, const uint8_t *esk, const uint8_t *ws) {
     MAYO_SIGN_VIEWS
     uint4 *masks = reinterpret_cast<uint4 *>(smem + C::off_masks);
@@ -149,7 +151,7 @@ __device__ __forceinline__ void sign_load_ws(uint8_t *smem, int tid, const uint8
 // Queue path: the CTA hashes itself (warp 0, warp-cooperative Keccak): digest = SHAKE256(M),
 // salt = SHAKE256(digest || 0^SK || seed_sk), t = SHAKE256(digest || salt), V || r for `ctr`
 // (sign.cu:225-252).  All threads must call it.
-template <int SET, int NT_>
+template <int SET, int NT_, bool CP_ = false>
 __device__ __forceinline__ void sign_hash_cta(uint8_t *smem, int tid, const uint8_t *esk, const uint8_t *msg,
                                               uint32_t mlen, int ctr) {
     MAYO_SIGN_VIEWS
@@ -191,7 +193,7 @@ __device__ __forceinline__ void sign_hash_cta(uint8_t *smem, int tid, const uint
 }
 
 // V || r for attempt `ctr` from the digest, salt and seed already in shared memory.
-template <int SET, int NT_>
+template <int SET, int NT_, bool CP_ = false>
 __device__ __forceinline__ void sign_next_vr(uint8_t *smem, int tid, int ctr) {
     MAYO_SIGN_VIEWS
     uint4 *masks = reinterpret_cast<uint4 *>(smem + C::off_masks);
@@ -222,8 +224,11 @@ __device__ __forceinline__ void sign_next_vr(uint8_t *smem, int tid, int ctr) {
 
 // One attempt on the V || r in shared memory: x on success, x = r on a singular system.
 // Returns whether the system had full rank (uniform over the CTA).  All threads must call it.
-template <int SET, int NT_>
-__device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8_t *esk) {
+// `pre`, when given, holds this attempt's T_j[r] = P1[r] V_j (rows r < v) and M_j[b] = V_j L[:, b]
+// (rows v + b) as bit-plane groups [j][row][w], computed for a whole batch on the tensor cores
+// (op_shared.cu); the two engine passes over P1 and L are then skipped.
+template <int SET, int NT_, bool CP_ = false>
+__device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8_t *esk, const uint4 *pre = nullptr) {
     MAYO_SIGN_VIEWS
     uint4 *masks = reinterpret_cast<uint4 *>(smem + C::off_masks);
     uint4 *bs = reinterpret_cast<uint4 *>(smem + C::off_bs);
@@ -256,7 +261,24 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
     __syncthreads();
 
     // ---- U = V^T P1 V ----
-    {
+    if (CP_ || pre) {  // a compact CTA has no engine staging: precomputed products only
+        // X[i][j] = sum_r V_i[r] T_j[r]: thread (j, w, rs) takes rows rs, rs + R, ...
+        constexpr int NROWS = S::v + S::o;
+        if (eng.active) {
+            G4 X[J];
+#pragma unroll
+            for (int i = 0; i < J; i++) X[i] = g4_zero();
+#pragma unroll 1
+            for (int r = eng.rs; r < S::v; r += R) {
+                const G4 T = g4_ld(pre + ((size_t)eng.j * NROWS + r) * W + eng.w);
+                const uint4 *mr = masks + (size_t)r * J;
+#pragma unroll
+                for (int i = 0; i < J; i++) g4_madd(X[i], T, mr[i]);
+            }
+#pragma unroll
+            for (int i = 0; i < J; i++) g4_atomic_xor(xacc + ((size_t)i * J + eng.j) * W + eng.w, X[i]);
+        }
+    } else {
         const P1Rows<SET> rows{P1};
         G4 X[J];
 #pragma unroll
@@ -310,7 +332,19 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
             }
         if (lane < NW) ypk[lane] = y ^ reinterpret_cast<const uint32_t *>(s_t)[lane];
     }
-    {
+    if (CP_ || pre) {  // a compact CTA has no engine staging: precomputed products only
+        constexpr int NROWS = S::v + S::o;
+        for (int idx = tid; idx < J * S::o * W; idx += NT) {
+            const int w = idx % W, jb = idx / W, b = jb % S::o, j = jb / S::o;
+            const uint4 pk = g4_to_packed(g4_ld(pre + ((size_t)j * NROWS + S::v + b) * W + w));
+            const uint32_t wd[4] = {pk.x, pk.y, pk.z, pk.w};
+            uint32_t *dst = mpk + ((size_t)j * S::o + b) * NW;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (4 * w + q < NW) dst[4 * w + q] = wd[q];
+        }
+        __syncthreads();
+    } else {
         const LColRows<SET> rows{L};
 #pragma unroll 1
         for (int b0 = 0; b0 < S::o; b0 += R) {
@@ -539,7 +573,7 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
 }
 
 // s = V + O x, then salt (sign.cu:147-191, 474-477).
-template <int SET, int NT_>
+template <int SET, int NT_, bool CP_ = false>
 __device__ __forceinline__ void sign_write(uint8_t *smem, int tid, const uint8_t *esk, uint8_t *sig) {
     MAYO_SIGN_VIEWS
     uint4 *masks = reinterpret_cast<uint4 *>(smem + C::off_masks);

@@ -53,9 +53,13 @@ __device__ __forceinline__ int pair_index(int i, int j, int k) { return i * k - 
 
 // Verify one instance; every thread of the CTA (NC + 32 of them) must call it.  Writes 0
 // (accept) or 1 (reject) to *res.  `smem` holds VerifyCfg<SET, NC>::total bytes.
+// `pre`, when given, holds T_j[r] = P[r] s_j for every row r < n as bit-plane groups [j][r][w],
+// computed for a whole batch on the tensor cores (op_shared.cu); the engine pass over the public
+// key is then skipped.
 template <int SET, int NC_>
 __device__ __forceinline__ void verify_instance(uint8_t *smem, int tid, const uint8_t *epk, const uint8_t *msg,
-                                                uint32_t mlen, const uint8_t *sig, uint8_t *res) {
+                                                uint32_t mlen, const uint8_t *sig, uint8_t *res,
+                                                const uint4 *pre = nullptr) {
     using S = Set<SET>;
     using C = VerifyCfg<SET, NC_>;
     constexpr int J = C::J, W = C::W, R = C::R, NC = C::NC, NW = C::NW;
@@ -97,18 +101,30 @@ __device__ __forceinline__ void verify_instance(uint8_t *smem, int tid, const ui
         G4 X[J];
 #pragma unroll
         for (int i = 0; i < J; i++) X[i] = g4_zero();
+        if (pre) {
+            if (eng.active) {
 #pragma unroll 1
-        for (int r0 = 0; r0 < S::n; r0 += R) {
-            eng.convert(rows, r0, S::n, tid, NC);
-            bar_sync(1, NC);
-            const int r = r0 + eng.rs;
-            if (eng.active && r < S::n) {
-                const G4 T = eng.row_product(rows, r);
-                const uint4 *mr = masks + (size_t)r * J;
+                for (int r = eng.rs; r < S::n; r += R) {
+                    const G4 T = g4_ld(pre + ((size_t)eng.j * S::n + r) * W + eng.w);
+                    const uint4 *mr = masks + (size_t)r * J;
 #pragma unroll
-                for (int i = 0; i < J; i++) g4_madd(X[i], T, mr[i]);
+                    for (int i = 0; i < J; i++) g4_madd(X[i], T, mr[i]);
+                }
             }
-            bar_sync(1, NC);
+        } else {
+#pragma unroll 1
+            for (int r0 = 0; r0 < S::n; r0 += R) {
+                eng.convert(rows, r0, S::n, tid, NC);
+                bar_sync(1, NC);
+                const int r = r0 + eng.rs;
+                if (eng.active && r < S::n) {
+                    const G4 T = eng.row_product(rows, r);
+                    const uint4 *mr = masks + (size_t)r * J;
+#pragma unroll
+                    for (int i = 0; i < J; i++) g4_madd(X[i], T, mr[i]);
+                }
+                bar_sync(1, NC);
+            }
         }
         if (eng.active) {
 #pragma unroll

@@ -147,6 +147,25 @@ MAYO_B200_API int mayo_b200_verify_many(int set, const uint8_t *epk, size_t epk_
                                         size_t mlen, const uint8_t *sig, size_t sig_stride, uint8_t *result,
                                         size_t batch, void *stream);
 
+/* ---- Extension (no counterpart in the reference): one key for the whole batch ----
+ * Same results as mayo_b200_sign_many / _verify_many with esk_stride / epk_stride 0, for batches
+ * signed or verified under a single expanded key.  The key's products with every instance's
+ * vectors (T = P1 V and M = V L for sign, T = P s for verify) run as one binary matrix product
+ * over the batch on the tensor cores (each GF(16) entry as its 4x4 bit matrix, sums mod 2);
+ * the rest of each operation runs per instance as in _many.  `ws` is device memory of
+ * mayo_b200_*_shared_ws_bytes(set, batch) bytes, 16-byte aligned; its first 4 bytes hold a
+ * status word after the call (0 = the tensor-core product ran; 1 = a bounded wait in it ran
+ * out and the per-instance engine produced the results instead). */
+MAYO_B200_API size_t mayo_b200_sign_shared_ws_bytes(int set, size_t batch);
+MAYO_B200_API int mayo_b200_sign_shared(int set, const uint8_t *esk, const uint8_t *msgs, const uint64_t *msg_off,
+                                        const uint32_t *msg_len, size_t msg_stride, size_t mlen, uint8_t *sig,
+                                        size_t sig_stride, uint8_t *ws, size_t batch, void *stream);
+MAYO_B200_API size_t mayo_b200_verify_shared_ws_bytes(int set, size_t batch);
+MAYO_B200_API int mayo_b200_verify_shared(int set, const uint8_t *epk, const uint8_t *msgs, const uint64_t *msg_off,
+                                          const uint32_t *msg_len, size_t msg_stride, size_t mlen, const uint8_t *sig,
+                                          size_t sig_stride, uint8_t *result, uint8_t *ws, size_t batch,
+                                          void *stream);
+
 /* ---- Extension (no counterpart in the reference): persistent work queue ----
  * A device queue of keypair / sign / verify items of all four parameter sets.  The mixed item
  * array is partitioned on the device (stably) into 12 buckets, one per (set, op), each drained by
