@@ -159,6 +159,7 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
     uint32_t *s_fail = s_tmem + 1;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int plane = warp & 3, half = warp >> 2;
+    const bool lead = lane == 0;
     const uint32_t inst0 = blockIdx.x * (uint32_t)P::NI;
 
     if (tid == 0) {
@@ -247,13 +248,11 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
             uint32_t r[32];
             tc::tmem_ld32(tbase + lane_base + (uint32_t)(b * N + col0), r);
             tc::tmem_wait_ld();
-            uint32_t mine = 0;
 #pragma unroll
             for (int q = 0; q < 32; q++) {
                 const uint32_t word = __ballot_sync(0xffffffffu, r[q] & 1u);
-                if (lane == q) mine = word;
+                if (lead) sTB[(col0 + q) * 4 + plane] = word;
             }
-            sTB[(col0 + lane) * 4 + plane] = mine;
         }
         tc::fence_before_sync();
         __syncthreads();

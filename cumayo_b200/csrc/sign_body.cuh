@@ -378,13 +378,18 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
 #pragma unroll
                 for (int q = 0; q < NW; q++) acc[q] ^= zshift_word<SET>(u, q, ell);
                 if (ell > 0) {
-                    // overflow coordinates m-ell..m-1 -> 0..ell-1, times z^n * c_n for n = 0..3
-                    uint32_t ov[NW];
+                    // overflow coordinates m-ell..m-1 -> 0..ell-1, times z^n * c_n for n = 0..3;
+                    // ell < k(k+1)/2, so only the first OVW packed words can hold overflow and
+                    // the fold (shifts by n < 4 coordinates) touches only the first FW words
+                    constexpr int ELL_MAX = S::k * (S::k + 1) / 2 - 1;
+                    constexpr int OVW = (ELL_MAX + 7) / 8 < NW ? (ELL_MAX + 7) / 8 : NW;
+                    constexpr int FW = OVW + 1 < NW ? OVW + 1 : NW;
+                    uint32_t ov[OVW];
 #pragma unroll
-                    for (int q = 0; q < NW; q++) ov[q] = zdown_word<SET>(u, q, S::m - ell);
+                    for (int q = 0; q < OVW; q++) ov[q] = zdown_word<SET>(u, q, S::m - ell);
                     // mask coordinates >= ell
 #pragma unroll
-                    for (int q = 0; q < NW; q++) {
+                    for (int q = 0; q < OVW; q++) {
                         const int lo = 8 * q;
                         if (lo >= ell) ov[q] = 0;
                         else if (lo + 8 > ell) ov[q] &= (1u << (4 * (ell - lo))) - 1;
@@ -394,8 +399,8 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
                         if (S::cf(n) == 0) continue;
                         uint32_t prev = 0;
 #pragma unroll
-                        for (int q = 0; q < NW; q++) {
-                            const uint32_t mc = nib8_mul_const(ov[q], S::cf(n));
+                        for (int q = 0; q < FW; q++) {
+                            const uint32_t mc = q < OVW ? nib8_mul_const(ov[q], S::cf(n)) : 0u;
                             acc[q] ^= n ? ((mc << (4 * n)) | (prev >> (32 - 4 * n))) : mc;
                             prev = mc;
                         }
