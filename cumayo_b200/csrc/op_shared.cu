@@ -42,7 +42,7 @@
 namespace mayo {
 
 constexpr uint32_t SH_SPIN = 1u << 22;  // mbarrier polls before a wait gives up
-constexpr size_t SH_SMEM_MAX = 220 * 1024;
+constexpr size_t SH_SMEM_MAX = 226 * 1024;
 constexpr int SH_GEMM_NT = 256;  // 8 warps: warp w reads TMEM lanes 32 (w % 4).., columns half w / 4
 constexpr int SH_FIX_CTAS = 2 * 148;
 
@@ -58,7 +58,7 @@ struct SharedProb {
     static constexpr int KSTEPS = KPAD / 32;                   // MMAs of K = 32 per tile
     static constexpr int NTILES = NROWS * W;
     static constexpr size_t TILE = (size_t)128 * KPAD;
-    static constexpr size_t smem_for(int N) { return (size_t)N * KPAD + 2 * TILE + (size_t)N * 16 + 64; }
+    static constexpr size_t smem_for(int N) { return (size_t)N * KPAD + 2 * TILE + 2 * (size_t)N * 16 + 64; }
     static constexpr int N = smem_for(256) <= SH_SMEM_MAX ? 256 : (smem_for(128) <= SH_SMEM_MAX ? 128 : 64);
     static constexpr int NI = N / S::k;  // instances per CTA
     static constexpr size_t SMEM = smem_for(N);
@@ -153,8 +153,8 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t *sB = smem;                                            // [KPAD/16][N][16]
     uint8_t *sA = smem + (size_t)N * KPAD;                          // 2 x [KPAD/16][128][16]
-    uint32_t *sTB = reinterpret_cast<uint32_t *>(sA + 2 * (size_t)TILE);  // [N][4] planes of one tile
-    uint64_t *bars = reinterpret_cast<uint64_t *>(sTB + 4 * N);    // full[2], mma_done[2]
+    uint32_t *sTB = reinterpret_cast<uint32_t *>(sA + 2 * (size_t)TILE);  // 2 x [N][4] planes of one tile
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sTB + 8 * N);    // full[2], mma_done[2]
     uint32_t *s_tmem = reinterpret_cast<uint32_t *>(bars + 4);
     uint32_t *s_fail = s_tmem + 1;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -241,30 +241,38 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
         // its A buffer is free: prefetch tile i + 2
         if (tid == 0 && done && i + 2 < NT) load(i + 2);
         // epilogue: bit 0 of each sum; warp (plane, half) reads plane `plane` (TMEM lanes
-        // 32 plane..) of columns [half N/2, (half + 1) N/2); one ballot = one 32-coordinate word
-#pragma unroll 1
-        for (int ch = 0; ch < N / 64; ch++) {
-            const int col0 = half * (N / 2) + ch * 32;
-            uint32_t r[32];
-            tc::tmem_ld32(tbase + lane_base + (uint32_t)(b * N + col0), r);
-            tc::tmem_wait_ld();
+        // 32 plane..) of columns [half N/2, (half + 1) N/2), all chunks before one wait; one
+        // ballot = one 32-coordinate word.  Staging alternates between two buffers, so one
+        // barrier per tile suffices (a buffer is rewritten only after the next tile's barrier).
+        {
+            constexpr int CH = N / 64;
+            uint32_t r[CH][32];
 #pragma unroll
-            for (int q = 0; q < 32; q++) {
-                const uint32_t word = __ballot_sync(0xffffffffu, r[q] & 1u);
-                if (lead) sTB[(col0 + q) * 4 + plane] = word;
+            for (int ch = 0; ch < CH; ch++)
+                tc::tmem_ld32(tbase + lane_base + (uint32_t)(b * N + half * (N / 2) + ch * 32), r[ch]);
+            tc::tmem_wait_ld();
+            uint32_t *tb = sTB + (size_t)b * 4 * N;
+#pragma unroll
+            for (int ch = 0; ch < CH; ch++) {
+                const int col0 = half * (N / 2) + ch * 32;
+#pragma unroll
+                for (int q = 0; q < 32; q++) {
+                    const uint32_t word = __ballot_sync(0xffffffffu, r[ch][q] & 1u);
+                    if (lead) tb[(col0 + q) * 4 + plane] = word;
+                }
             }
         }
         tc::fence_before_sync();
         __syncthreads();
         const int rr = i / W, w = i - rr * W;
+        const uint32_t *tb = sTB + (size_t)b * 4 * N;
         for (int n = tid; n < P::NI * S::k; n += SH_GEMM_NT) {
             const uint32_t inst = inst0 + (uint32_t)(n / S::k);
             const int j = n % S::k;
             if (inst < batch)
                 planes[(size_t)inst * P::PLANES + ((size_t)j * P::NROWS + rr) * W + w] =
-                    *reinterpret_cast<const uint4 *>(sTB + 4 * n);
+                    *reinterpret_cast<const uint4 *>(tb + 4 * n);
         }
-        __syncthreads();
     }
     // unwind: no bulk copy or MMA of this CTA may still be in flight when TMEM is freed
     if (tid == 0) {

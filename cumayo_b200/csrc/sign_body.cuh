@@ -424,22 +424,24 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
     for (int i = tid; i < W * 4; i += NT) reinterpret_cast<uint32_t *>(rhsacc)[i] = 0;
     __syncthreads();
 
-    // ---- Gauss-Jordan in constant time.  Thread owns columns c = tid + NT*q. ----
+    // ---- Gauss-Jordan in constant time.  Thread owns columns c = KO - (tid + NT q): the RHS on
+    // thread 0 and the columns still to update (c > pc) on the lowest threads, so the work of a
+    // step stays in as few warps as possible. ----
     G4 col[CPT][W];
     uint32_t rr[CPT];
 #pragma unroll
     for (int q = 0; q < CPT; q++) {
-        const int c = tid + NT * q;
+        const int c = KO - (tid + NT * q);
 #pragma unroll
-        for (int w = 0; w < W; w++) col[q][w] = c < C::NCOL ? g4_ld(acol + (size_t)c * W + w) : g4_zero();
+        for (int w = 0; w < W; w++) col[q][w] = c >= 0 ? g4_ld(acol + (size_t)c * W + w) : g4_zero();
         const int rn = S::k * S::m;  // r starts after the k V-vectors (sign.cu:250)
-        rr[q] = c < KO ? (s_vr[(rn + c) >> 1] >> (((rn + c) & 1) * 4)) & 0xF : 0u;
+        rr[q] = (c >= 0 && c < KO) ? (s_vr[(rn + c) >> 1] >> (((rn + c) & 1) * 4)) & 0xF : 0u;
     }
     // y <- y - A r  (sample_solution, sign.cu:36-45)
 #pragma unroll
     for (int q = 0; q < CPT; q++) {
-        const int c = tid + NT * q;
-        if (c < KO) {
+        const int c = KO - (tid + NT * q);
+        if (c >= 0 && c < KO) {
             const uint4 mk = scalar_masks(rr[q]);
 #pragma unroll
             for (int w = 0; w < W; w++) {
@@ -452,7 +454,7 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < CPT; q++)
-        if (tid + NT * q == KO)
+        if (tid + NT * q == 0)  // the RHS column
 #pragma unroll
             for (int w = 0; w < W; w++) col[q][w] = g4_xor(col[q][w], g4_ld(rhsacc + w));
 
@@ -474,7 +476,7 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
         uint32_t *ohw = reinterpret_cast<uint32_t *>(buf + W);  // oh[0..W), found at [7]
 #pragma unroll
         for (int q = 0; q < CPT; q++) {
-            if (tid + NT * q != pc) continue;
+            if (KO - (tid + NT * q) != pc) continue;
             uint32_t oh[W], found = 0;
 #pragma unroll
             for (int w = 0; w < W; w++) {
@@ -522,8 +524,7 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
         }
 #pragma unroll
         for (int q = 0; q < CPT; q++) {
-            const int c = tid + NT * q;
-            if (c <= pc || c >= C::NCOL) continue;
+            if (KO - (tid + NT * q) <= pc) continue;
             uint32_t e0 = 0, e1 = 0, e2 = 0, e3 = 0;
 #pragma unroll
             for (int w = 0; w < W; w++) {
@@ -549,14 +550,14 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
     // publish the reduced RHS; x = r + z (z_c = rhs[p(c)] on pivot columns)
 #pragma unroll
     for (int q = 0; q < CPT; q++)
-        if (tid + NT * q == KO)
+        if (tid + NT * q == 0)  // the RHS column
 #pragma unroll
             for (int w = 0; w < W; w++) g4_st(rhsacc + w, col[q][w]);  // not a buffer still being read
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < CPT; q++) {
-        const int c = tid + NT * q;
-        if (c < KO) {
+        const int c = KO - (tid + NT * q);
+        if (c >= 0 && c < KO) {
             uint32_t z0 = 0, z1 = 0, z2 = 0, z3 = 0;
 #pragma unroll
             for (int w = 0; w < W; w++) {
@@ -596,31 +597,55 @@ __device__ __forceinline__ void sign_write(uint8_t *smem, int tid, const uint8_t
     uint8_t *s_x = smem + C::off_xs;
     int *s_flag = reinterpret_cast<int *>(smem + C::off_flag);
     (void)masks; (void)bs; (void)acol; (void)xacc; (void)upk; (void)mpk; (void)pivbuf; (void)rhsacc; (void)ypk; (void)s_key; (void)s_t; (void)s_vr; (void)s_x; (void)s_flag;
+    // s_i = V_i + O x_i on bit planes: the columns of O as planes (the engine staging area, free
+    // after the attempt), then per (i, group w) o multiply-accumulates; nibbles staged one per
+    // byte (the mask area, also free) because s_i starts mid-byte when n is odd.
     const uint8_t *O_g = esk + S::sk;
-    uint8_t *sigp = sig;
-    for (int bidx = tid; bidx < S::k * S::n / 2; bidx += NT) {
-        uint32_t nb[2];
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int e = 2 * bidx + h, i = e / S::n, t = e - i * S::n;
-            uint32_t val;
+    uint4 *ocol = reinterpret_cast<uint4 *>(smem + C::off_bs);  // [o][W]
+    uint8_t *snib = smem + C::off_masks;                           // [k * n]
+    static_assert((size_t)S::o * W * 16 <= (C::sz_bs > C::sz_acol ? C::sz_bs : C::sz_acol), "O planes fit");
+    static_assert((size_t)S::k * S::n <= (size_t)S::v * J * 16, "nibble staging fits");
+    for (int idx = tid; idx < S::o * W; idx += NT) {
+        const int q = idx / W, w = idx - q * W;
+        uint32_t pk[4] = {0u, 0u, 0u, 0u};
+#pragma unroll 4
+        for (int e = 0; e < 32; e++) {
+            const int t = 32 * w + e;
             if (t < S::m) {
-                uint32_t acc = 0;
-#pragma unroll
-                for (int q = 0; q < S::o; q++) {
-                    const int oi = t * S::o + q;
-                    const uint32_t ov = (O_g[oi >> 1] >> ((oi & 1) * 4)) & 0xF;
-                    acc ^= gf16_mul_ct(ov, s_x[i * S::o + q]);
-                }
-                const int vi = i * S::m + t;
-                val = ((s_vr[vi >> 1] >> ((vi & 1) * 4)) & 0xF) ^ acc;
-            } else {
-                val = s_x[i * S::o + (t - S::m)];
+                const int oi = t * S::o + q;
+                pk[e >> 3] |= (uint32_t)((O_g[oi >> 1] >> ((oi & 1) * 4)) & 0xF) << (4 * (e & 7));
             }
-            nb[h] = val;
         }
-        sigp[bidx] = (uint8_t)(nb[0] | (nb[1] << 4));
+        g4_st(ocol + idx, g4_from_packed(pk[0], pk[1], pk[2], pk[3]));
     }
+    for (int idx = tid; idx < S::k * S::o; idx += NT) {  // x_i: the last o nibbles of s_i
+        const int i = idx / S::o, q = idx - i * S::o;
+        snib[i * S::n + S::m + q] = s_x[idx];
+    }
+    __syncthreads();
+    for (int idx = tid; idx < S::k * W; idx += NT) {
+        const int i = idx / W, w = idx - i * W;
+        // V_i group w: packed nibbles i * m + 32 w .. (m even, so byte aligned)
+        const uint8_t *vb = s_vr + (i * S::m + 32 * w) / 2;
+        const int nb = min(16, (S::m - 32 * w + 1) / 2);
+        uint32_t pk[4] = {0u, 0u, 0u, 0u};
+        for (int bb = 0; bb < nb; bb++) pk[bb >> 2] |= (uint32_t)vb[bb] << (8 * (bb & 3));
+        if (S::m - 32 * w < 32 && ((S::m - 32 * w) & 1)) {  // odd tail: drop the extra nibble
+            const int last = S::m - 32 * w;
+            pk[last >> 3] &= ~(0xFu << (4 * (last & 7)));
+        }
+        G4 acc = g4_from_packed(pk[0], pk[1], pk[2], pk[3]);
+#pragma unroll 1
+        for (int q = 0; q < S::o; q++) g4_madd(acc, g4_ld(ocol + q * W + w), scalar_masks(s_x[i * S::o + q]));
+        const uint4 u = g4_to_packed(acc);
+        const uint32_t wd[4] = {u.x, u.y, u.z, u.w};
+        for (int e = 0; e < 32 && 32 * w + e < S::m; e++)
+            snib[i * S::n + 32 * w + e] = (uint8_t)((wd[e >> 3] >> (4 * (e & 7))) & 0xF);
+    }
+    __syncthreads();
+    uint8_t *sigp = sig;
+    for (int bidx = tid; bidx < S::k * S::n / 2; bidx += NT)
+        sigp[bidx] = (uint8_t)(snib[2 * bidx] | (snib[2 * bidx + 1] << 4));
     for (int i = tid; i < S::sk; i += NT) sigp[S::k * S::n / 2 + i] = s_key[S::digest + i];
 }
 
