@@ -178,6 +178,19 @@ __device__ __forceinline__ void g4_atomic_xor(uint4 *dst, const G4 &g) {
 
 // Named barrier over the first `n` threads (n a multiple of 32).
 __device__ __forceinline__ void bar_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+// Named barrier that also returns the OR of `pred` over the participating threads (uniform).
+__device__ __forceinline__ bool bar_red_or(int id, int n, bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(id), "r"(n)
+        : "memory");
+    return r != 0;
+}
 
 // ---------------------------------------------------------------------------------------------
 // z * y mod f(z) on a packed m-vector held one 32-bit word (8 coordinates) per lane, lanes

@@ -43,7 +43,8 @@ namespace mayo {
 
 constexpr uint32_t SH_SPIN = 1u << 22;  // mbarrier polls before a wait gives up
 constexpr size_t SH_SMEM_MAX = 226 * 1024;
-constexpr int SH_GEMM_NT = 256;  // 8 warps: warp w reads TMEM lanes 32 (w % 4).., columns half w / 4
+constexpr int SH_EPI_NT = 256;              // 8 epilogue warps: warp w reads TMEM lanes 32 (w % 4).., half w / 4
+constexpr int SH_GEMM_NT = SH_EPI_NT + 32;  // + one producer warp (loads, MMA issue)
 constexpr int SH_FIX_CTAS = 2 * 148;
 
 // The product for sign (rows: T_j[r] over P1 for r < v, then M_j[b] over L) or verify (rows
@@ -58,10 +59,16 @@ struct SharedProb {
     static constexpr int KSTEPS = KPAD / 32;                   // MMAs of K = 32 per tile
     static constexpr int NTILES = NROWS * W;
     static constexpr size_t TILE = (size_t)128 * KPAD;
-    static constexpr size_t smem_for(int N) { return (size_t)N * KPAD + 2 * TILE + 2 * (size_t)N * 16 + 64; }
-    static constexpr int N = smem_for(256) <= SH_SMEM_MAX ? 256 : (smem_for(128) <= SH_SMEM_MAX ? 128 : 64);
-    static constexpr int NI = N / S::k;  // instances per CTA
-    static constexpr size_t SMEM = smem_for(N);
+    // instance vectors (NINST columns, resident) + STAGES key tiles + barriers
+    static constexpr size_t smem_for(int ni, int st) { return (size_t)ni * KPAD + (size_t)st * TILE + 128; }
+    static constexpr int NINST = smem_for(256, 2) <= SH_SMEM_MAX ? 256 : 128;  // vector columns per CTA
+    static constexpr int STAGES = smem_for(NINST, 4) <= SH_SMEM_MAX   ? 4
+                                  : smem_for(NINST, 3) <= SH_SMEM_MAX ? 3
+                                  : smem_for(NINST, 2) <= SH_SMEM_MAX ? 2
+                                                                      : 1;
+    static constexpr int NB = NINST / 128;  // MMA M-blocks of 128 vector columns
+    static constexpr int NI = NINST / S::k; // instances per CTA
+    static constexpr size_t SMEM = smem_for(NINST, STAGES);
     static constexpr size_t PLANES = (size_t)S::k * NROWS * W;  // uint4 per instance
     // first column c that can be nonzero in row rr
     __host__ __device__ static constexpr int c_min(int rr) { return VERIFY ? rr : (rr < S::v ? rr : 0); }
@@ -106,8 +113,9 @@ struct SharedWs {
     static size_t retry_off(size_t batch) { return a + a_bytes + batch * (inst + planes); }
 };
 
-// A, tiled: tile tt = rr * W + w holds rows rho = 32 b + t' (bit plane b, lane t'; lane t' carries
-// coordinate 32 w + 8 (t' & 3) + (t' >> 2), the bit order of a G4 plane) and K bytes 4 c + b';
+// A, tiled: tile tt = rr * W + w holds rows rho = 32 b + q (bit plane b; row q carries coordinate
+// 32 w + cq(q), cq(q) = 8 ((q >> 2) & 3) + 2 (q & 3) + (q >> 4), the order in which the epilogue's
+// packing of 32 sums lands each coordinate on its bit of a G4 plane) and K bytes 4 c + b';
 // layout [K / 16][128 rows][16 bytes].  One thread per 16 bytes.  Also resets the control words.
 template <int SET, bool VERIFY>
 __global__ void shared_a_kernel(const uint8_t *key, uint8_t *A, uint32_t *ctl) {
@@ -121,7 +129,7 @@ __global__ void shared_a_kernel(const uint8_t *key, uint8_t *A, uint32_t *ctl) {
     const int rem = (int)(idx - (size_t)tt * per_tile);
     const int ch = rem / 128, rho = rem - ch * 128;
     const int rr = tt / P::W, w = tt - rr * P::W, b = rho >> 5, tp = rho & 31;
-    const int t = 32 * w + 8 * (tp & 3) + (tp >> 2);
+    const int t = 32 * w + 8 * ((tp >> 2) & 3) + 2 * (tp & 3) + (tp >> 4);
     uint32_t wd[4] = {0u, 0u, 0u, 0u};
     if (t < S::m) {
 #pragma unroll
@@ -139,41 +147,69 @@ __global__ void shared_a_kernel(const uint8_t *key, uint8_t *A, uint32_t *ctl) {
         make_uint4(wd[0], wd[1], wd[2], wd[3]);
 }
 
+// Bit 0 of 32 sums packed into one word: bit 8 j + k <- sum 4 k + j (three byte permutes per
+// four sums, then the low bits merged; the A tile's row order makes this a G4 plane).
+__device__ __forceinline__ uint32_t pack_lsb32(const uint32_t (&r)[32]) {
+    uint32_t x = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const uint32_t lo = __byte_perm(r[4 * k], r[4 * k + 1], 0x0040);
+        const uint32_t hi = __byte_perm(r[4 * k + 2], r[4 * k + 3], 0x0040);
+        x += (__byte_perm(lo, hi, 0x5410) & 0x01010101u) << k;  // disjoint bits: + is |
+    }
+    return x;
+}
+
 // vec: instance i's vectors start at vec + i * vec_stride, entry c of vector j is nibble
 // j * NVEC + c.  planes: instance i at planes + i * PLANES, [j][row][w].
+//
+// The MMA puts the vector columns on M (TMEM lanes) and the 128 rows of a key tile on N, so each
+// epilogue thread owns one vector column and reads the 32 sums of one bit plane of its tile
+// from its own TMEM lane: packing them into the plane's word is thread-local.
+//
+// Warp-specialized: warp 8 (one thread) is the producer -- it keeps STAGES key tiles in flight
+// (bulk copies), issues each tile's MMAs into one of two TMEM accumulators once that accumulator
+// has been read out, and refills a stage once the MMAs that read it completed; warps 0-7 are
+// the epilogue -- they wait for a tile's MMAs, read their sums (tcgen05.ld), hand the
+// accumulator back (acc_free), pack and store.  Barriers: full[stage] (copy landed),
+// mma_done[acc] (commit), acc_free[acc] (8 arrivals).
 template <int SET, bool VERIFY>
 __global__ void __launch_bounds__(SH_GEMM_NT, 1)
     shared_gemm_kernel(const uint8_t *__restrict__ A, const uint8_t *__restrict__ vec, size_t vec_stride,
                        uint4 *__restrict__ planes, uint32_t batch, uint32_t *ctl) {
     using P = SharedProb<SET, VERIFY>;
     using S = Set<SET>;
-    constexpr int N = P::N, KPAD = P::KPAD, NT = P::NTILES, W = P::W;
+    constexpr int NIN = P::NINST, KPAD = P::KPAD, NT = P::NTILES, W = P::W, ST = P::STAGES, NB = P::NB;
     constexpr uint32_t TILE = (uint32_t)P::TILE;
-    constexpr uint32_t IDESC = tc::idesc_u8(128, N);
+    constexpr uint32_t IDESC = tc::idesc_u8(128, 128);
+    constexpr uint32_t ACC = 128 * NB;  // TMEM columns of one accumulator
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t *sB = smem;                                            // [KPAD/16][N][16]
-    uint8_t *sA = smem + (size_t)N * KPAD;                          // 2 x [KPAD/16][128][16]
-    uint32_t *sTB = reinterpret_cast<uint32_t *>(sA + 2 * (size_t)TILE);  // 2 x [N][4] planes of one tile
-    uint64_t *bars = reinterpret_cast<uint64_t *>(sTB + 8 * N);    // full[2], mma_done[2]
-    uint32_t *s_tmem = reinterpret_cast<uint32_t *>(bars + 4);
+    uint8_t *sB = smem;                                            // [KPAD/16][NIN][16] vector columns
+    uint8_t *sA = smem + (size_t)NIN * KPAD;                        // ST x [KPAD/16][128][16] key tiles
+    uint64_t *full = reinterpret_cast<uint64_t *>(sA + (size_t)ST * TILE);  // [ST]
+    uint64_t *mma_done = full + ST;                                 // [2]
+    uint64_t *acc_free = mma_done + 2;                              // [2]
+    uint32_t *s_tmem = reinterpret_cast<uint32_t *>(acc_free + 2);
     uint32_t *s_fail = s_tmem + 1;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int plane = warp & 3, half = warp >> 2;
-    const bool lead = lane == 0;
     const uint32_t inst0 = blockIdx.x * (uint32_t)P::NI;
 
     if (tid == 0) {
-        for (int i = 0; i < 4; i++) tc::mbar_init(&bars[i], 1);
+        for (int i = 0; i < ST; i++) tc::mbar_init(&full[i], 1);
+        for (int i = 0; i < 2; i++) {
+            tc::mbar_init(&mma_done[i], 1);
+            tc::mbar_init(&acc_free[i], SH_EPI_NT / 32);
+        }
         tc::fence_mbar_init();
         *s_fail = 0;
     }
     if (warp == 0) {
-        tc::tmem_alloc(s_tmem, 2 * N);
+        tc::tmem_alloc(s_tmem, 2 * ACC);
         tc::tmem_relinquish();
     }
-    // B: column n = (instance n / k, vector j = n % k); K byte 4 c + b' = bit b' of entry c
-    for (int idx = tid; idx < (KPAD / 16) * N; idx += SH_GEMM_NT) {
-        const int ch = idx / N, n = idx - ch * N;
+    // vector columns: column n = (instance n / k, vector j = n % k); K byte 4 c + b' = bit b' of entry c
+    for (int idx = tid; idx < (KPAD / 16) * NIN; idx += SH_GEMM_NT) {
+        const int ch = idx / NIN, n = idx - ch * NIN;
         const uint32_t inst = inst0 + (uint32_t)(n / S::k);
         const int j = n % S::k;
         uint32_t wd[4] = {0u, 0u, 0u, 0u};
@@ -189,106 +225,113 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
                 }
             }
         }
-        *reinterpret_cast<uint4 *>(sB + ((size_t)ch * N + n) * 16) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+        *reinterpret_cast<uint4 *>(sB + ((size_t)ch * NIN + n) * 16) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
     }
     tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tbase = *s_tmem;
-    const uint32_t sA_addr = tc::smem_u32(sA), sB_addr = tc::smem_u32(sB);
 
-    // thread 0's bookkeeping of asynchronous work, for the unwind after a timeout
-    uint32_t ld_issued[2] = {0u, 0u}, ld_waited[2] = {0u, 0u}, mma_issued[2] = {0u, 0u}, mma_waited[2] = {0u, 0u};
-    auto load = [&](int tile) {
-        const int b = tile & 1;
-        tc::mbar_arrive_expect_tx(&bars[b], TILE);
-        tc::bulk_g2s(sA + (size_t)b * TILE, A + (size_t)tile * TILE, TILE, &bars[b]);
-        ld_issued[b]++;
-    };
-    auto issue = [&](int tile) -> bool {
-        const int b = tile & 1;
-        if (!tc::mbar_wait(&bars[b], ld_waited[b] & 1u, SH_SPIN)) return false;
-        ld_waited[b]++;
-        tc::fence_after_sync();
-        const int s0 = P::c_min(tile / W) / 8;  // K bytes 32 s .. 32 s + 31 hold columns 8 s .. 8 s + 7
-        for (int s = s0; s < P::KSTEPS; s++) {
-            const uint64_t ad = tc::desc_kmajor(sA_addr + (uint32_t)b * TILE + (uint32_t)s * 4096u, 2048u, 128u);
-            const uint64_t bd = tc::desc_kmajor(sB_addr + (uint32_t)s * 2u * N * 16u, (uint32_t)N * 16u, 128u);
-            tc::mma_i8(tbase + (uint32_t)b * N, ad, bd, IDESC, s > s0 ? 1u : 0u);
-        }
-        tc::mma_commit(&bars[2 + b]);
-        mma_issued[b]++;
-        return true;
-    };
-
-    if (tid == 0) {
-        load(0);
-        if (NT > 1) load(1);
-        if (!issue(0)) *s_fail = 1;
-    }
-    __syncthreads();
-    const uint32_t lane_base = (uint32_t)(plane * 32) << 16;
+    if (warp == SH_EPI_NT / 32) {
+        // ---------------- producer ----------------
+        if (lane == 0) {
+            const uint32_t sA_addr = tc::smem_u32(sA), sB_addr = tc::smem_u32(sB);
+            int last_load[ST];  // last tile loaded into each stage (for the unwind)
+            for (int st = 0; st < ST; st++) last_load[st] = -1;
+            int consumed = -1, committed = -1;
+            auto load = [&](int tile) {
+                const int st = tile % ST;
+                tc::mbar_arrive_expect_tx(&full[st], TILE);
+                tc::bulk_g2s(sA + (size_t)st * TILE, A + (size_t)tile * TILE, TILE, &full[st]);
+                last_load[st] = tile;
+            };
+            for (int t = 0; t < ST && t < NT; t++) load(t);
+            bool ok = true;
 #pragma unroll 1
-    for (int i = 0; i < NT && !*s_fail; i++) {
-        const int b = i & 1;
-        if (tid == 0 && i + 1 < NT && !issue(i + 1)) atomicOr(s_fail, 1u);
-        // the MMAs of tile i
-        const bool done = tc::mbar_wait(&bars[2 + b], (uint32_t)(i >> 1) & 1u, SH_SPIN);
-        if (!done) atomicOr(s_fail, 1u);
-        if (tid == 0 && done) mma_waited[b]++;
-        tc::fence_after_sync();
-        // its A buffer is free: prefetch tile i + 2
-        if (tid == 0 && done && i + 2 < NT) load(i + 2);
-        // epilogue: bit 0 of each sum; warp (plane, half) reads plane `plane` (TMEM lanes
-        // 32 plane..) of columns [half N/2, (half + 1) N/2), all chunks before one wait; one
-        // ballot = one 32-coordinate word.  Staging alternates between two buffers, so one
-        // barrier per tile suffices (a buffer is rewritten only after the next tile's barrier).
-        {
-            constexpr int CH = N / 64;
-            uint32_t r[CH][32];
+            for (int i = 0; i < NT && ok; i++) {
+                const int st = i % ST, b = i & 1;
+                ok = tc::mbar_wait(&full[st], (uint32_t)(i / ST) & 1u, SH_SPIN);
+                if (ok) consumed = i;
+                if (ok && i >= 2) ok = tc::mbar_wait(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, SH_SPIN);
+                if (!ok) break;
+                tc::fence_after_sync();
+                const int s0 = P::c_min(i / W) / 8;  // K bytes 32 s .. 32 s + 31 hold columns 8 s .. 8 s + 7
+                for (int s = s0; s < P::KSTEPS; s++) {
+                    const uint64_t kd =
+                        tc::desc_kmajor(sA_addr + (uint32_t)st * TILE + (uint32_t)s * 4096u, 2048u, 128u);
 #pragma unroll
-            for (int ch = 0; ch < CH; ch++)
-                tc::tmem_ld32(tbase + lane_base + (uint32_t)(b * N + half * (N / 2) + ch * 32), r[ch]);
-            tc::tmem_wait_ld();
-            uint32_t *tb = sTB + (size_t)b * 4 * N;
-#pragma unroll
-            for (int ch = 0; ch < CH; ch++) {
-                const int col0 = half * (N / 2) + ch * 32;
-#pragma unroll
-                for (int q = 0; q < 32; q++) {
-                    const uint32_t word = __ballot_sync(0xffffffffu, r[ch][q] & 1u);
-                    if (lead) tb[(col0 + q) * 4 + plane] = word;
+                    for (int h = 0; h < NB; h++) {
+                        const uint64_t vd = tc::desc_kmajor(sB_addr + (uint32_t)s * 2u * NIN * 16u + (uint32_t)h * 2048u,
+                                                            (uint32_t)NIN * 16u, 128u);
+                        tc::mma_i8(tbase + (uint32_t)b * ACC + (uint32_t)h * 128u, vd, kd, IDESC, s > s0 ? 1u : 0u);
+                    }
                 }
+                tc::mma_commit(&mma_done[b]);
+                committed = i;
+                // refill: with several stages, the stage of tile i - 1 (free once its MMAs
+                // completed, while tile i's run); with one stage, tile i's own after its MMAs
+                constexpr int D = ST > 1 ? 1 : 0;
+                if (i >= D && i - D + ST < NT) {
+                    ok = tc::mbar_wait(&mma_done[(i - D) & 1], (uint32_t)((i - D) >> 1) & 1u, SH_SPIN);
+                    if (ok) load(i - D + ST);
+                }
+                if (*reinterpret_cast<volatile uint32_t *>(s_fail)) ok = false;
             }
+            if (!ok) atomicOr(s_fail, 1u);
+            // unwind: no copy or MMA of this CTA may be in flight when TMEM is freed
+            for (int st = 0; st < ST; st++)
+                if (last_load[st] > consumed) tc::mbar_wait(&full[st], (uint32_t)(last_load[st] / ST) & 1u, SH_SPIN);
+            if (committed >= 0) tc::mbar_wait(&mma_done[committed & 1], (uint32_t)(committed >> 1) & 1u, SH_SPIN);
         }
-        tc::fence_before_sync();
-        __syncthreads();
-        const int rr = i / W, w = i - rr * W;
-        const uint32_t *tb = sTB + (size_t)b * 4 * N;
-        for (int n = tid; n < P::NI * S::k; n += SH_GEMM_NT) {
-            const uint32_t inst = inst0 + (uint32_t)(n / S::k);
-            const int j = n % S::k;
-            if (inst < batch)
-                planes[(size_t)inst * P::PLANES + ((size_t)j * P::NROWS + rr) * W + w] =
-                    *reinterpret_cast<const uint4 *>(tb + 4 * n);
+    } else {
+        // ---------------- epilogue ----------------
+        // warp: TMEM lanes 32 (warp % 4).. = vector columns; with two M-blocks warps 0-3 / 4-7 take
+        // block 0 / 1 and all four planes, with one block they take planes 0-1 / 2-3
+        constexpr int PL = NB == 2 ? 4 : 2;
+        const int grp = warp & 3;
+        const int h = NB == 2 ? (warp >> 2) : 0;
+        const int pl0 = NB == 2 ? 0 : 2 * (warp >> 2);
+        const int n = h * 128 + grp * 32 + lane;  // this thread's vector column
+        const uint32_t inst = inst0 + (uint32_t)(n / S::k);
+        const int j = n % S::k;
+        const bool live = n < P::NI * S::k && inst < batch;
+        uint4 *dst = planes + (size_t)inst * P::PLANES + (size_t)j * P::NROWS * W;
+        const uint32_t taddr = tbase + ((uint32_t)(grp * 32) << 16) + (uint32_t)h * 128u + (uint32_t)pl0 * 32u;
+#pragma unroll 1
+        for (int i = 0; i < NT; i++) {
+            const int b = i & 1;
+            if (!tc::mbar_wait(&mma_done[b], (uint32_t)(i >> 1) & 1u, SH_SPIN)) {
+                atomicOr(s_fail, 1u);
+                break;
+            }
+            tc::fence_after_sync();
+            uint32_t r[PL][32];
+#pragma unroll
+            for (int p = 0; p < PL; p++) tc::tmem_ld32(taddr + (uint32_t)b * ACC + (uint32_t)p * 32u, r[p]);
+            tc::tmem_wait_ld();
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&acc_free[b]);  // the accumulator may be overwritten now
+            uint32_t wd[PL];
+#pragma unroll
+            for (int p = 0; p < PL; p++) wd[p] = pack_lsb32(r[p]);
+            if (live) {
+                uint32_t *o = reinterpret_cast<uint32_t *>(dst + i);  // tile i = (row i / W, group i % W)
+                if (PL == 4)
+                    *reinterpret_cast<uint4 *>(o) = make_uint4(wd[0], wd[PL > 1 ? 1 : 0], wd[PL > 2 ? 2 : 0], wd[PL > 3 ? 3 : 0]);
+                else
+                    *reinterpret_cast<uint2 *>(o + pl0) = make_uint2(wd[0], wd[PL > 1 ? 1 : 0]);
+            }
+            if (*reinterpret_cast<volatile uint32_t *>(s_fail)) break;
         }
-    }
-    // unwind: no bulk copy or MMA of this CTA may still be in flight when TMEM is freed
-    if (tid == 0) {
-        for (int b = 0; b < 2; b++) {
-            while (ld_waited[b] < ld_issued[b] && tc::mbar_wait(&bars[b], ld_waited[b] & 1u, SH_SPIN)) ld_waited[b]++;
-            while (mma_waited[b] < mma_issued[b] &&
-                   tc::mbar_wait(&bars[2 + b], mma_waited[b] & 1u, SH_SPIN))
-                mma_waited[b]++;
-        }
-        if (*s_fail) atomicOr(ctl, 1u);
     }
     tc::fence_before_sync();
     __syncthreads();
+    if (tid == 0 && *s_fail) atomicOr(ctl, 1u);
     if (warp == 0) {
         tc::fence_after_sync();
-        tc::tmem_dealloc(tbase, 2 * N);
+        tc::tmem_dealloc(tbase, 2 * ACC);
     }
 }
 
