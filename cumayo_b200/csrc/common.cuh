@@ -402,6 +402,28 @@ __host__ __device__ __forceinline__ uint32_t gf16_inv_ct(uint32_t a) {
     return gf16_mul_ct(gf16_mul_ct(a2, a4), a8);
 }
 
+// Inverses of 0..15 as one 64-bit constant (nibble a = a^-1, 0^-1 := 0).  Read with a shift by
+// 4a: no memory access and no branch, so constant time in a.
+__host__ __device__ constexpr uint32_t gf16_mul_cx(uint32_t a, uint32_t b) {
+    uint32_t r = 0;
+    for (int i = 0; i < 4; i++)
+        if (b & (1u << i)) r ^= a << i;
+    for (int d = 6; d >= 4; d--)
+        if (r & (1u << d)) r ^= 0x13u << (d - 4);  // x^4 = x + 1
+    return r;
+}
+__host__ __device__ constexpr uint64_t gf16_inv_table() {
+    uint64_t t = 0;
+    for (uint32_t a = 1; a < 16; a++)
+        for (uint32_t b = 1; b < 16; b++)
+            if (gf16_mul_cx(a, b) == 1) t |= (uint64_t)b << (4 * a);
+    return t;
+}
+constexpr uint64_t kGf16InvTable = gf16_inv_table();
+__host__ __device__ __forceinline__ uint32_t gf16_inv_reg(uint32_t a) {
+    return (uint32_t)(kGf16InvTable >> (4 * (a & 0xF))) & 0xFu;
+}
+
 // Multiply the eight packed nibbles of a word by a public constant c (0..15).
 __host__ __device__ __forceinline__ uint32_t nib8_mul_const(uint32_t w, uint32_t c) {
     uint32_t r = 0, t = w;

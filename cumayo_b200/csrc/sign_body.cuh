@@ -468,63 +468,70 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
 #pragma unroll
         for (int w = 0; w < W; w++) my_oh[q][w] = 0;
     }
+    // The owner of a column computes its pivot (lowest unpivoted row with a nonzero entry), the
+    // inverse and F' = inv * (a + e_p), and publishes F' and the row one-hot in buffer pcx & 1.
+    auto publish = [&](int q, int pcx) {
+        uint4 *buf = pivbuf + (pcx & 1) * (W + 2);
+        uint32_t *ohw = reinterpret_cast<uint32_t *>(buf + W);  // oh[0..W), found at [7]
+        uint32_t oh[W], found = 0;
+#pragma unroll
+        for (int w = 0; w < W; w++) {
+            const G4 &a = col[q][w];
+            const uint32_t nz = (a.p0 | a.p1 | a.p2 | a.p3) & ~pivoted[w];
+            const uint32_t low = nz & (0u - nz);
+            oh[w] = low & ~found;
+            found |= 0u - (uint32_t)(nz != 0u);
+        }
+        uint32_t o0 = 0, o1 = 0, o2 = 0, o3 = 0;
+#pragma unroll
+        for (int w = 0; w < W; w++) {
+            o0 |= col[q][w].p0 & oh[w];
+            o1 |= col[q][w].p1 & oh[w];
+            o2 |= col[q][w].p2 & oh[w];
+            o3 |= col[q][w].p3 & oh[w];
+        }
+        const uint32_t piv = (uint32_t)(o0 != 0) | ((uint32_t)(o1 != 0) << 1) | ((uint32_t)(o2 != 0) << 2) |
+                             ((uint32_t)(o3 != 0) << 3);
+        const uint4 inv_m = scalar_masks(gf16_inv_reg(piv) & found);
+#pragma unroll
+        for (int w = 0; w < W; w++) {
+            G4 ap = col[q][w];
+            ap.p0 ^= oh[w];
+            G4 F = g4_zero();
+            g4_madd(F, ap, inv_m);
+            g4_st(buf + w, F);
+            ohw[w] = oh[w];
+            my_oh[q][w] = oh[w];
+        }
+        ohw[7] = found;
+        my_has[q] = found;
+    };
+#pragma unroll
+    for (int q = 0; q < CPT; q++)
+        if (KO - (tid + NT * q) == 0) publish(q, 0);
+    __syncthreads();
 #pragma unroll 1
     for (int pc = 0; pc < KO; pc++) {
-        // The owner of column pc computes the pivot (lowest unpivoted row with a nonzero
-        // entry), its inverse and F' = inv * (a + e_p), and publishes F' and the row one-hot.
-        uint4 *buf = pivbuf + (pc & 1) * (W + 2);
-        uint32_t *ohw = reinterpret_cast<uint32_t *>(buf + W);  // oh[0..W), found at [7]
-#pragma unroll
-        for (int q = 0; q < CPT; q++) {
-            if (KO - (tid + NT * q) != pc) continue;
-            uint32_t oh[W], found = 0;
-#pragma unroll
-            for (int w = 0; w < W; w++) {
-                const G4 &a = col[q][w];
-                const uint32_t nz = (a.p0 | a.p1 | a.p2 | a.p3) & ~pivoted[w];
-                const uint32_t low = nz & (0u - nz);
-                oh[w] = low & ~found;
-                found |= 0u - (uint32_t)(nz != 0u);
-            }
-            uint32_t o0 = 0, o1 = 0, o2 = 0, o3 = 0;
-#pragma unroll
-            for (int w = 0; w < W; w++) {
-                o0 |= col[q][w].p0 & oh[w];
-                o1 |= col[q][w].p1 & oh[w];
-                o2 |= col[q][w].p2 & oh[w];
-                o3 |= col[q][w].p3 & oh[w];
-            }
-            const uint32_t piv = (uint32_t)(o0 != 0) | ((uint32_t)(o1 != 0) << 1) |
-                                 ((uint32_t)(o2 != 0) << 2) | ((uint32_t)(o3 != 0) << 3);
-            const uint4 inv_m = scalar_masks(gf16_inv_ct(piv) & found);
-#pragma unroll
-            for (int w = 0; w < W; w++) {
-                G4 ap = col[q][w];
-                ap.p0 ^= oh[w];
-                G4 F = g4_zero();
-                g4_madd(F, ap, inv_m);
-                g4_st(buf + w, F);
-                ohw[w] = oh[w];
-                my_oh[q][w] = oh[w];
-            }
-            ohw[7] = found;
-            my_has[q] = found;
-        }
-        __syncthreads();
-        // every column right of pc: col ^= col[p] * F'  (eliminates row p elsewhere, normalises
+        // Every column right of pc: col ^= col[p] * F'  (eliminates row p elsewhere, normalises
         // row p).  A column left of pc is already a unit vector e_p' (or has no entry in an
-        // unpivoted row), so col[p] = 0 there for every later pivot row p and the update would be
-        // a no-op; skipping it depends only on the public loop index.
+        // unpivoted row), so col[p] = 0 there for every later pivot row p and the update would
+        // be a no-op; skipping it depends only on the public loop index.  Lookahead: the owner
+        // of column pc + 1 publishes its pivot right after its own update, while the other
+        // columns update, so each step needs one barrier and the owner's chain overlaps them.
+        const uint4 *buf = pivbuf + (pc & 1) * (W + 2);
+        const uint32_t *ohw = reinterpret_cast<const uint32_t *>(buf + W);
         G4 F[W];
         uint32_t oh[W];
 #pragma unroll
         for (int w = 0; w < W; w++) {
             F[w] = g4_ld(buf + w);
             oh[w] = ohw[w];
+            pivoted[w] |= oh[w];
         }
 #pragma unroll
         for (int q = 0; q < CPT; q++) {
-            if (KO - (tid + NT * q) <= pc) continue;
+            const int c = KO - (tid + NT * q);
+            if (c <= pc) continue;
             uint32_t e0 = 0, e1 = 0, e2 = 0, e3 = 0;
 #pragma unroll
             for (int w = 0; w < W; w++) {
@@ -533,14 +540,13 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
                 e2 |= col[q][w].p2 & oh[w];
                 e3 |= col[q][w].p3 & oh[w];
             }
-            const uint32_t ev = (uint32_t)(e0 != 0) | ((uint32_t)(e1 != 0) << 1) | ((uint32_t)(e2 != 0) << 2) |
-                                ((uint32_t)(e3 != 0) << 3);
-            const uint4 em = scalar_masks(ev);
+            const uint4 em = make_uint4(0u - (uint32_t)(e0 != 0), 0u - (uint32_t)(e1 != 0), 0u - (uint32_t)(e2 != 0),
+                                        0u - (uint32_t)(e3 != 0));
 #pragma unroll
             for (int w = 0; w < W; w++) g4_madd(col[q][w], F[w], em);
+            if (c == pc + 1 && c < KO) publish(q, c);
         }
-#pragma unroll
-        for (int w = 0; w < W; w++) pivoted[w] |= oh[w];
+        __syncthreads();
     }
     // rank test (sign.cu:107-115 rejects when the last echelon row is zero, i.e. rank < m)
     int rank = 0;

@@ -24,6 +24,7 @@ int main() {
         for (uint32_t b = 0; b < 16; b++)
             if (gf16_mul_ct(a, b) != ref_mul(a, b)) FAIL("gf16_mul_ct %u %u", a, b);
         if (a && ref_mul(a, gf16_inv_ct(a)) != 1) FAIL("gf16_inv_ct %u", a);
+        if (gf16_inv_reg(a) != gf16_inv_ct(a)) FAIL("gf16_inv_reg %u", a);
     }
     if (gf16_inv_ct(0) != 0) FAIL("inv(0)");
     for (int it = 0; it < 2000; it++) {
