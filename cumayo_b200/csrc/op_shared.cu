@@ -57,18 +57,26 @@ struct SharedProb {
     static constexpr int NROWS = VERIFY ? S::n : S::v + S::o;  // m-vector rows of the result
     static constexpr int KPAD = (4 * NVEC + 31) / 32 * 32;    // bytes of one B column (K)
     static constexpr int KSTEPS = KPAD / 32;                   // MMAs of K = 32 per tile
-    static constexpr int NTILES = NROWS * W;
-    static constexpr size_t TILE = (size_t)128 * KPAD;
-    // instance vectors (NINST columns, resident) + STAGES key tiles + barriers
-    static constexpr size_t smem_for(int ni, int st) { return (size_t)ni * KPAD + (size_t)st * TILE + 128; }
-    static constexpr int NINST = smem_for(256, 2) <= SH_SMEM_MAX ? 256 : 128;  // vector columns per CTA
-    static constexpr int STAGES = smem_for(NINST, 4) <= SH_SMEM_MAX   ? 4
-                                  : smem_for(NINST, 3) <= SH_SMEM_MAX ? 3
-                                  : smem_for(NINST, 2) <= SH_SMEM_MAX ? 2
-                                                                      : 1;
+    static constexpr int NGROUPS = NROWS * W;  // 128-row groups of the key matrix (row rr, group w)
+    // One MMA: M = 128 vector columns (NB blocks), N = KROWS = 128 G key rows (G groups per tile);
+    // an accumulator takes NB * KROWS <= 256 TMEM columns (two of them: double-buffered).  Larger
+    // MMAs first, as shared memory allows: (G 2, 128 columns), (G 1, 256 columns), (G 1, 128).
+    static constexpr size_t smem_cfg(int g, int ni, int st) {
+        return (size_t)ni * KPAD + (size_t)st * g * 128 * KPAD + 128;
+    }
+    static constexpr int G = smem_cfg(2, 128, 2) <= SH_SMEM_MAX ? 2 : 1;
+    static constexpr int NINST = G == 2 ? 128 : (smem_cfg(1, 256, 2) <= SH_SMEM_MAX ? 256 : 128);
+    static constexpr int STAGES = smem_cfg(G, NINST, 4) <= SH_SMEM_MAX   ? 4
+                                  : smem_cfg(G, NINST, 3) <= SH_SMEM_MAX ? 3
+                                  : smem_cfg(G, NINST, 2) <= SH_SMEM_MAX ? 2
+                                                                          : 1;
+    static constexpr int KROWS = 128 * G;
+    static constexpr int NTILES = (NGROUPS + G - 1) / G;
+    static constexpr size_t TILE = (size_t)KROWS * KPAD;
     static constexpr int NB = NINST / 128;  // MMA M-blocks of 128 vector columns
     static constexpr int NI = NINST / S::k; // instances per CTA
-    static constexpr size_t SMEM = smem_for(NINST, STAGES);
+    static constexpr size_t SMEM = smem_cfg(G, NINST, STAGES);
+    static_assert(NB * KROWS <= 256, "accumulator columns");
     static constexpr size_t PLANES = (size_t)S::k * NROWS * W;  // uint4 per instance
     // first column c that can be nonzero in row rr
     __host__ __device__ static constexpr int c_min(int rr) { return VERIFY ? rr : (rr < S::v ? rr : 0); }
@@ -113,25 +121,26 @@ struct SharedWs {
     static size_t retry_off(size_t batch) { return a + a_bytes + batch * (inst + planes); }
 };
 
-// A, tiled: tile tt = rr * W + w holds rows rho = 32 b + q (bit plane b; row q carries coordinate
+// A, tiled: group gi = rr * W + w holds rows rho = 32 b + q (bit plane b; row q carries coordinate
 // 32 w + cq(q), cq(q) = 8 ((q >> 2) & 3) + 2 (q & 3) + (q >> 4), the order in which the epilogue's
-// packing of 32 sums lands each coordinate on its bit of a G4 plane) and K bytes 4 c + b';
-// layout [K / 16][128 rows][16 bytes].  One thread per 16 bytes.  Also resets the control words.
+// packing of 32 sums lands each coordinate on its bit of a G4 plane) and K bytes 4 c + b'; a
+// tile is G consecutive groups, layout [K / 16][G * 128 rows][16 bytes].  One thread per 16
+// bytes.  Also resets the control words.
 template <int SET, bool VERIFY>
 __global__ void shared_a_kernel(const uint8_t *key, uint8_t *A, uint32_t *ctl) {
     using P = SharedProb<SET, VERIFY>;
     using S = Set<SET>;
-    constexpr size_t per_tile = (size_t)(P::KPAD / 16) * 128;
+    constexpr size_t per_group = (size_t)(P::KPAD / 16) * 128;
     const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx < 2) ctl[idx] = 0;
-    if (idx >= (size_t)P::NTILES * per_tile) return;
-    const int tt = (int)(idx / per_tile);
-    const int rem = (int)(idx - (size_t)tt * per_tile);
+    if (idx >= (size_t)P::NTILES * P::G * per_group) return;
+    const int gi = (int)(idx / per_group);  // group (the last tile's second group may be padding)
+    const int rem = (int)(idx - (size_t)gi * per_group);
     const int ch = rem / 128, rho = rem - ch * 128;
-    const int rr = tt / P::W, w = tt - rr * P::W, b = rho >> 5, tp = rho & 31;
+    const int rr = gi / P::W, w = gi - rr * P::W, b = rho >> 5, tp = rho & 31;
     const int t = 32 * w + 8 * ((tp >> 2) & 3) + 2 * (tp & 3) + (tp >> 4);
     uint32_t wd[4] = {0u, 0u, 0u, 0u};
-    if (t < S::m) {
+    if (gi < P::NGROUPS && t < S::m) {
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const int c = 4 * ch + q;
@@ -143,7 +152,8 @@ __global__ void shared_a_kernel(const uint8_t *key, uint8_t *A, uint32_t *ctl) {
             wd[q] = v;
         }
     }
-    *reinterpret_cast<uint4 *>(A + (size_t)tt * P::TILE + (size_t)ch * 2048 + (size_t)rho * 16) =
+    const int tile = gi / P::G, g = gi - tile * P::G;
+    *reinterpret_cast<uint4 *>(A + (size_t)tile * P::TILE + (size_t)ch * P::KROWS * 16 + (size_t)(g * 128 + rho) * 16) =
         make_uint4(wd[0], wd[1], wd[2], wd[3]);
 }
 
@@ -179,13 +189,14 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
                        uint4 *__restrict__ planes, uint32_t batch, uint32_t *ctl) {
     using P = SharedProb<SET, VERIFY>;
     using S = Set<SET>;
-    constexpr int NIN = P::NINST, KPAD = P::KPAD, NT = P::NTILES, W = P::W, ST = P::STAGES, NB = P::NB;
+    constexpr int NIN = P::NINST, KPAD = P::KPAD, NT = P::NTILES, ST = P::STAGES, NB = P::NB, G = P::G;
+    constexpr int KR = P::KROWS;
     constexpr uint32_t TILE = (uint32_t)P::TILE;
-    constexpr uint32_t IDESC = tc::idesc_u8(128, 128);
-    constexpr uint32_t ACC = 128 * NB;  // TMEM columns of one accumulator
+    constexpr uint32_t IDESC = tc::idesc_u8(128, KR);
+    constexpr uint32_t ACC = KR * NB;  // TMEM columns of one accumulator
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t *sB = smem;                                            // [KPAD/16][NIN][16] vector columns
-    uint8_t *sA = smem + (size_t)NIN * KPAD;                        // ST x [KPAD/16][128][16] key tiles
+    uint8_t *sA = smem + (size_t)NIN * KPAD;                        // ST x [KPAD/16][KR][16] key tiles
     uint64_t *full = reinterpret_cast<uint64_t *>(sA + (size_t)ST * TILE);  // [ST]
     uint64_t *mma_done = full + ST;                                 // [2]
     uint64_t *acc_free = mma_done + 2;                              // [2]
@@ -256,15 +267,17 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
                 if (ok && i >= 2) ok = tc::mbar_wait(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, SH_SPIN);
                 if (!ok) break;
                 tc::fence_after_sync();
-                const int s0 = P::c_min(i / W) / 8;  // K bytes 32 s .. 32 s + 31 hold columns 8 s .. 8 s + 7
+                // K bytes 32 s .. 32 s + 31 hold columns 8 s .. 8 s + 7; the tile's first group has
+                // the smallest row, so the smallest first nonzero column
+                const int s0 = P::c_min((i * G) / P::W) / 8;
                 for (int s = s0; s < P::KSTEPS; s++) {
-                    const uint64_t kd =
-                        tc::desc_kmajor(sA_addr + (uint32_t)st * TILE + (uint32_t)s * 4096u, 2048u, 128u);
+                    const uint64_t kd = tc::desc_kmajor(sA_addr + (uint32_t)st * TILE + (uint32_t)s * 2u * KR * 16u,
+                                                        (uint32_t)KR * 16u, 128u);
 #pragma unroll
                     for (int h = 0; h < NB; h++) {
                         const uint64_t vd = tc::desc_kmajor(sB_addr + (uint32_t)s * 2u * NIN * 16u + (uint32_t)h * 2048u,
                                                             (uint32_t)NIN * 16u, 128u);
-                        tc::mma_i8(tbase + (uint32_t)b * ACC + (uint32_t)h * 128u, vd, kd, IDESC, s > s0 ? 1u : 0u);
+                        tc::mma_i8(tbase + (uint32_t)b * ACC + (uint32_t)h * KR, vd, kd, IDESC, s > s0 ? 1u : 0u);
                     }
                 }
                 tc::mma_commit(&mma_done[b]);
@@ -286,18 +299,21 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
         }
     } else {
         // ---------------- epilogue ----------------
-        // warp: TMEM lanes 32 (warp % 4).. = vector columns; with two M-blocks warps 0-3 / 4-7 take
-        // block 0 / 1 and all four planes, with one block they take planes 0-1 / 2-3
-        constexpr int PL = NB == 2 ? 4 : 2;
-        const int grp = warp & 3;
-        const int h = NB == 2 ? (warp >> 2) : 0;
-        const int pl0 = NB == 2 ? 0 : 2 * (warp >> 2);
+        // warp: TMEM lanes 32 (warp % 4).. = vector columns.  Warps 0-3 / 4-7 split the work:
+        // two M-blocks -> block 0 / 1, all four planes; two groups per tile -> group 0 / 1;
+        // otherwise planes 0-1 / 2-3.
+        constexpr int PL = (NB == 2 || G == 2) ? 4 : 2;
+        const int grp = warp & 3, half = warp >> 2;
+        const int h = NB == 2 ? half : 0;
+        const int g = G == 2 ? half : 0;
+        const int pl0 = PL == 4 ? 0 : 2 * half;
         const int n = h * 128 + grp * 32 + lane;  // this thread's vector column
         const uint32_t inst = inst0 + (uint32_t)(n / S::k);
         const int j = n % S::k;
         const bool live = n < P::NI * S::k && inst < batch;
-        uint4 *dst = planes + (size_t)inst * P::PLANES + (size_t)j * P::NROWS * W;
-        const uint32_t taddr = tbase + ((uint32_t)(grp * 32) << 16) + (uint32_t)h * 128u + (uint32_t)pl0 * 32u;
+        uint4 *dst = planes + (size_t)inst * P::PLANES + (size_t)j * P::NROWS * P::W;
+        const uint32_t taddr =
+            tbase + ((uint32_t)(grp * 32) << 16) + (uint32_t)(h * KR + g * 128) + (uint32_t)pl0 * 32u;
 #pragma unroll 1
         for (int i = 0; i < NT; i++) {
             const int b = i & 1;
@@ -316,8 +332,9 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
             uint32_t wd[PL];
 #pragma unroll
             for (int p = 0; p < PL; p++) wd[p] = pack_lsb32(r[p]);
-            if (live) {
-                uint32_t *o = reinterpret_cast<uint32_t *>(dst + i);  // tile i = (row i / W, group i % W)
+            const int gi = i * G + g;  // group = (row gi / W, coordinate group gi % W)
+            if (live && gi < P::NGROUPS) {
+                uint32_t *o = reinterpret_cast<uint32_t *>(dst + gi);
                 if (PL == 4)
                     *reinterpret_cast<uint4 *>(o) = make_uint4(wd[0], wd[PL > 1 ? 1 : 0], wd[PL > 2 ? 2 : 0], wd[PL > 3 ? 3 : 0]);
                 else
@@ -516,7 +533,7 @@ static int launch_product(const uint8_t *key, const uint8_t *vec, size_t vec_str
     using WSL = SharedWs<SET, VERIFY>;
     uint32_t *ctl = reinterpret_cast<uint32_t *>(ws);
     uint8_t *A = ws + WSL::a;
-    const size_t a_threads = (size_t)P::NTILES * (P::KPAD / 16) * 128;
+    const size_t a_threads = (size_t)P::NTILES * P::G * (P::KPAD / 16) * 128;
     shared_a_kernel<SET, VERIFY><<<(unsigned)((a_threads + 255) / 256), 256, 0, st>>>(key, A, ctl);
     if (!set_smem_attr(shared_gemm_kernel<SET, VERIFY>, P::SMEM)) return ST_CUDA;
     uint4 *planes = reinterpret_cast<uint4 *>(ws + WSL::planes_off(batch));
