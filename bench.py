@@ -44,8 +44,33 @@ def _hbm_peak() -> tuple[float, str]:
 
 
 HBM_PEAK_GBS, HBM_PEAK_SRC = _hbm_peak()
+
+
+def _bf16_peak() -> tuple[float, str]:
+    """Measured dense bf16 GEMM throughput (burst), TFLOP/s, else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return 1590.0, "fallback"
+
+
+BF16_PEAK_TFLOPS, BF16_PEAK_SRC = _bf16_peak()
 LOP3_LANE_OPS_PER_CLK_SM = 64  # measured on this pool's B200 (profiles/int_pipes_b200.md)
 A128 = lambda x: (x + 127) // 128 * 128  # noqa: E731
+KERNEL_ROOF_DEF = {
+    "alu": "algorithmic ops = 0.5 x the GF(16) MACs the kernel owns (16 LOP3 per 32 MACs) / kernel time; "
+           "peak = measured LOP3 issue rate 64 lane-ops/clk/SM x 148 SMs x median SM clock",
+    "tensor": "algorithmic ops = 2 x 16 binary MACs per GF(16) MAC of the key products / kernel time; "
+              "peak = 2 x measured dense bf16 GEMM (int8 rate of the tensor cores)",
+    "hbm": "algorithmic bytes read + written / kernel time; peak = measured copy bandwidth",
+}
+# DRAM bytes per instance (dram__bytes_read.sum + dram__bytes_write.sum of one launch / its
+# instances) from one ncu capture of the MAYO_2 shared-key kernels at 16,384 instances
+# (profiles/sign_tail_mayo2_shared_b16384.md, profiles/product_gemm_mayo2_shared_b16384.md);
+# the traffic grows in proportion to the instances, so a launch's traffic is this x its batch.
+KERNEL_TRAFFIC_PER_INST = {2: {"sign.tail": 179.924224e6 / 16384, "verify.tail": 177.24288e6 / 16384,
+                               "sign.product": 125.610752e6 / 16384, "verify.product": 126.423552e6 / 16384}}
 
 # ---------------------------------------------------------------------------------------------
 # workloads
@@ -196,6 +221,7 @@ def run_ours(args, dist: Dist):
     launches_per_step = 0
     seed = 1 + dist.rank
     plain_fn = None
+    kernel_profile = None
     plain_api = "per-(set, op) batched launches: keypair_from_seed, sign_many, verify_many"
     plain_check = None
 
@@ -271,6 +297,37 @@ def run_ours(args, dist: Dist):
                "api": "mayo_b200_sign_shared / verify_shared (key products on the tensor cores)"}
         expected = np.zeros(batch, np.uint8)
         res_dev = lambda: res  # noqa: E731
+        # Per-kernel algorithmic work (per call of `batch` instances) for the rooflines:
+        #   product: GF(16) MACs of the key products done as binary MACs on the tensor cores
+        #            (16 bit-products per GF(16) MAC, 2 ops each, int8 peak = 2 x bf16);
+        #   tail:    the per-instance GF(16) MACs left to the integer pipes (0.5 lane-op each);
+        #   hash:    bytes read and written in HBM.
+        n_, m_, o_, k_ = PARAMS[s]
+        v_ = n_ - o_
+        e1_, e2_, e3_ = v_ * (v_ + 1) // 2, v_ * o_, o_ * (o_ + 1) // 2
+        prod_macs = {"sign": k_ * m_ * e1_ + k_ * m_ * v_ * o_, "verify": k_ * m_ * (e1_ + e2_ + e3_)}
+        tail_macs = {"sign": m_ * k_ * k_ * v_ + m_ * m_ * (k_ * o_ + 1), "verify": m_ * k_ * k_ * n_}
+        kernel_model = {}
+        for ph in ("sign", "verify"):
+            kernel_model[(ph, "product")] = ("tensor", 32.0 * prod_macs[ph] * batch)
+            kernel_model[(ph, "tail")] = ("alu", 0.5 * tail_macs[ph] * batch)
+            kernel_model[(ph, "hash")] = ("hbm", float(body.nbytes + offs.nbytes + lens.nbytes +
+                                                      batch * (z.sig_bytes if ph == "verify" else 0) + 64 * batch))
+
+        def kernel_profile(steps):
+            """Per-kernel times inside the shared-key calls (CUDA events between the kernels)."""
+            acc = {}
+            M.Mayo.shared_timing(True)
+            try:
+                for _ in range(steps):
+                    flush.fill_(1)
+                    for ph, fn in phases:
+                        fn()
+                        for kname, ms in M.Mayo.shared_timing_read().items():
+                            acc[(ph, kname)] = acc.get((ph, kname), 0.0) + ms
+            finally:
+                M.Mayo.shared_timing(False)
+            return {key: v / steps for key, v in acc.items()}
     elif wl["kind"] == "keypair_sign_verify":
         # every instance: seeded keypair -> sign (compact sk, expanded inside) -> verify (compact pk)
         mlen = wl["mlen"][0]
@@ -489,6 +546,43 @@ def run_ours(args, dist: Dist):
     # The binding roof: distinct-key verify streams every EPK from HBM (bound hbm); the other
     # workloads keep keys L2-resident and are integer-ALU bound (bound alu).
     out["roofline"] = dict(out["roofline_hbm"] if wl["kind"] == "distinct_verify" else out["roofline_alu"])
+    if kernel_profile is not None:
+        kt = kernel_profile(args.steps)
+        int8_peak = 2.0 * BF16_PEAK_TFLOPS
+
+        def traffic(name):
+            per = KERNEL_TRAFFIC_PER_INST.get(s, {}).get(name)
+            return None if per is None else int(per * batch)
+        kern = {}
+        for key, ms in sorted(kt.items()):
+            ent = {"ms": round(ms, 4), "share": round(ms / sum(kt.values()), 4)}
+            if key in kernel_model and ms > 0:
+                bound, amount = kernel_model[key]
+                if bound == "tensor":
+                    a_ = amount / (ms / 1e3) / 1e12
+                    ent.update(bound="tensor", achieved=round(a_, 1), peak=round(int8_peak, 1), unit="Tops/s",
+                               frac=round(a_ / int8_peak, 4))
+                elif bound == "alu":
+                    a_ = amount / (ms / 1e3) / 1e9
+                    ent.update(bound="alu", achieved=round(a_, 1), peak=round(peak_ops, 1), unit="G int-ops/s",
+                               frac=round(a_ / peak_ops, 4))
+                else:
+                    a_ = amount / (ms / 1e3) / 1e9
+                    ent.update(bound="hbm", achieved=round(a_, 1), peak=HBM_PEAK_GBS, unit="GB/s",
+                               frac=round(a_ / HBM_PEAK_GBS, 4))
+            kern[f"{key[0]}.{key[1]}"] = ent
+        out["kernels"] = kern
+        top = max(kt, key=kt.get)
+        t = kern[f"{top[0]}.{top[1]}"]
+        out["roofline"] = {"bound": t.get("bound"), "kernel": f"{top[0]} {top[1]} kernel ({args.workload})",
+                           "achieved": t.get("achieved"), "peak": t.get("peak"), "unit": t.get("unit"),
+                           "frac": t.get("frac"), "traffic": traffic(f"{top[0]}.{top[1]}"),
+                           "definition": KERNEL_ROOF_DEF[t.get("bound")]}
+        pr = kern.get("sign.product", {})
+        out["roofline_tensor"] = {"bound": "tensor", "kernel": f"sign product kernel ({args.workload})",
+                                  "achieved": pr.get("achieved"), "peak": pr.get("peak"), "unit": "Tops/s",
+                                  "frac": pr.get("frac"), "traffic": traffic("sign.product"),
+                                  "definition": KERNEL_ROOF_DEF["tensor"]}
     if plain_fn is not None:
         # the same work as per-(set, op) batched launches on the same GPU
         for _ in range(args.warmup):

@@ -101,6 +101,10 @@ def lib() -> ctypes.CDLL:
         L.mayo_b200_sign_shared.argtypes = [ctypes.c_int, vp, vp, vp, vp, sz, sz, vp, sz, vp, sz, vp]
         L.mayo_b200_verify_shared.restype = ctypes.c_int
         L.mayo_b200_verify_shared.argtypes = [ctypes.c_int, vp, vp, vp, vp, sz, sz, vp, sz, vp, vp, sz, vp]
+        L.mayo_b200_shared_timing.restype = ctypes.c_int
+        L.mayo_b200_shared_timing.argtypes = [ctypes.c_int]
+        L.mayo_b200_shared_timing_read.restype = ctypes.c_int
+        L.mayo_b200_shared_timing_read.argtypes = [ctypes.POINTER(ctypes.c_float)]
         _lib = L
     return _lib
 
@@ -323,6 +327,21 @@ class Mayo:
                                              msg_stride, mlen, _ptr(sig),
                                              z.sig_bytes if sig_stride is None else sig_stride, _ptr(result),
                                              _ptr(ws), batch, _stream(stream)), "verify_shared")
+
+    SHARED_KERNELS = ("hash", "key_tiles", "product", "tail", "fixup")
+
+    @staticmethod
+    def shared_timing(enable: bool) -> None:
+        """Profiling aid: record per-kernel CUDA events inside sign_shared / verify_shared calls
+        made from this thread while enabled."""
+        _check(lib().mayo_b200_shared_timing(1 if enable else 0), "shared_timing")
+
+    @staticmethod
+    def shared_timing_read() -> dict:
+        """Milliseconds of each kernel of the last recorded sign_shared / verify_shared call."""
+        buf = (ctypes.c_float * 5)()
+        _check(lib().mayo_b200_shared_timing_read(buf), "shared_timing_read")
+        return dict(zip(Mayo.SHARED_KERNELS, (float(x) for x in buf)))
 
     def sign_noalloc_max_batch(self) -> int:
         return int(lib().mayo_b200_sign_noalloc_max_batch(self.set))

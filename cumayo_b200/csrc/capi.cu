@@ -378,6 +378,14 @@ MAYO_B200_API int mayo_b200_sign_shared(int set, const uint8_t *esk, const uint8
     return kernel_rc(mayo::launch_sign_shared(set, io, ws, batch, S_(stream)));
 }
 
+MAYO_B200_API int mayo_b200_shared_timing(int enable) { return kernel_rc(mayo::shared_timing(enable)); }
+
+MAYO_B200_API int mayo_b200_shared_timing_read(float *ms) {
+    if (!ms) return MAYO_B200_ERR_ARG;
+    const int rc = mayo::shared_timing_read(ms);
+    return rc == mayo::ST_OK ? MAYO_B200_OK : (rc == mayo::ST_BAD_ARG ? MAYO_B200_ERR_ARG : MAYO_B200_ERR_CUDA);
+}
+
 MAYO_B200_API size_t mayo_b200_verify_shared_ws_bytes(int set, size_t batch) {
     return mayo::shared_ws_bytes(set, true, batch);
 }

@@ -525,6 +525,17 @@ __global__ void __launch_bounds__(VerifyCfg<SET>::NT)
     }
 }
 
+// ---- optional per-kernel timing (profiling aid, off by default; per host thread) ----
+struct ShTiming {
+    bool on = false, ready = false;
+    cudaEvent_t ev[6];
+    int n = 0;
+};
+thread_local ShTiming tl_tm;
+static void tmark(cudaStream_t st) {
+    if (tl_tm.on && tl_tm.ready && tl_tm.n < 6) cudaEventRecord(tl_tm.ev[tl_tm.n++], st);
+}
+
 // ---- launchers ----
 template <int SET, bool VERIFY>
 static int launch_product(const uint8_t *key, const uint8_t *vec, size_t vec_stride, uint8_t *ws, size_t batch,
@@ -535,10 +546,12 @@ static int launch_product(const uint8_t *key, const uint8_t *vec, size_t vec_str
     uint8_t *A = ws + WSL::a;
     const size_t a_threads = (size_t)P::NTILES * P::G * (P::KPAD / 16) * 128;
     shared_a_kernel<SET, VERIFY><<<(unsigned)((a_threads + 255) / 256), 256, 0, st>>>(key, A, ctl);
+    tmark(st);
     if (!set_smem_attr(shared_gemm_kernel<SET, VERIFY>, P::SMEM)) return ST_CUDA;
     uint4 *planes = reinterpret_cast<uint4 *>(ws + WSL::planes_off(batch));
     shared_gemm_kernel<SET, VERIFY><<<(unsigned)((batch + P::NI - 1) / P::NI), SH_GEMM_NT, P::SMEM, st>>>(
         A, vec, vec_stride, planes, (uint32_t)batch, ctl);
+    tmark(st);
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
 }
 
@@ -553,7 +566,10 @@ static int sign_shared_t(const SignIO &io0, uint8_t *ws, size_t batch, cudaStrea
     io.esk_stride = 0;
     io.ws = ws + WSL::inst_off();
     io.ws_stride = WSL::inst;
+    tl_tm.n = 0;
+    tmark(st);
     int rc = launch_sign_hash(SET, io, batch, st);
+    tmark(st);
     if (rc != ST_OK) return rc;
     rc = launch_product<SET, false>(io.esk, io.ws + SignWs<SET>::vr, io.ws_stride, ws, batch, st);
     if (rc != ST_OK) return rc;
@@ -563,9 +579,11 @@ static int sign_shared_t(const SignIO &io0, uint8_t *ws, size_t batch, cudaStrea
     sign_shared_tail_kernel<SET><<<(unsigned)batch, CT::NT, CT::total, st>>>(
         io.esk, io.sig, io.sig_stride, io.ws, io.ws_stride, reinterpret_cast<const uint4 *>(ws + WSL::planes_off(batch)),
         ctl, retry);
+    tmark(st);
     if (!set_smem_attr(sign_shared_fix_kernel<SET>, CF::total)) return ST_CUDA;
     sign_shared_fix_kernel<SET><<<fix_grid(batch), CF::NT, CF::total, st>>>(io.esk, io.sig, io.sig_stride, io.ws,
                                                                             io.ws_stride, ctl, retry, (uint32_t)batch);
+    tmark(st);
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
 }
 
@@ -577,15 +595,20 @@ static int verify_shared_t(const VerifyIO &io0, uint8_t *ws, size_t batch, cudaS
     VerifyIO io = io0;
     io.epk_stride = 0;
     uint8_t *tws = ws + WSL::inst_off();
+    tl_tm.n = 0;
+    tmark(st);
     verify_hash_kernel<SET><<<(unsigned)((batch + 127) / 128), 128, 0, st>>>(io, tws, WSL::inst, (uint32_t)batch);
+    tmark(st);
     int rc = launch_product<SET, true>(io.epk, io.sig, io.sig_stride, ws, batch, st);
     if (rc != ST_OK) return rc;
     const uint32_t *ctl = reinterpret_cast<const uint32_t *>(ws);
     if (!set_smem_attr(verify_shared_tail_kernel<SET>, CT::total)) return ST_CUDA;
     verify_shared_tail_kernel<SET><<<(unsigned)batch, CT::NT, CT::total, st>>>(
         io, tws, WSL::inst, reinterpret_cast<const uint4 *>(ws + WSL::planes_off(batch)), ctl);
+    tmark(st);
     if (!set_smem_attr(verify_shared_fix_kernel<SET>, CF::total)) return ST_CUDA;
     verify_shared_fix_kernel<SET><<<fix_grid(batch), CF::NT, CF::total, st>>>(io, ctl, (uint32_t)batch);
+    tmark(st);
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
 }
 
@@ -597,6 +620,25 @@ size_t shared_ws_bytes(int set, bool verify, size_t batch) {
         case 5: return verify ? SharedWs<5, true>::bytes(batch) : SharedWs<5, false>::bytes(batch);
         default: return 0;
     }
+}
+
+int shared_timing(int enable) {
+    if (enable && !tl_tm.ready) {
+        for (int i = 0; i < 6; i++)
+            if (cudaEventCreate(&tl_tm.ev[i]) != cudaSuccess) return ST_CUDA;
+        tl_tm.ready = true;
+    }
+    tl_tm.on = enable != 0;
+    tl_tm.n = 0;
+    return ST_OK;
+}
+
+int shared_timing_read(float *ms) {
+    if (!tl_tm.ready || tl_tm.n != 6) return ST_BAD_ARG;
+    if (cudaEventSynchronize(tl_tm.ev[5]) != cudaSuccess) return ST_CUDA;
+    for (int i = 0; i < 5; i++)
+        if (cudaEventElapsedTime(&ms[i], tl_tm.ev[i], tl_tm.ev[i + 1]) != cudaSuccess) return ST_CUDA;
+    return ST_OK;
 }
 
 int launch_sign_shared(int set, const SignIO &io, uint8_t *ws, size_t batch, cudaStream_t st) {

@@ -76,5 +76,7 @@ size_t sign_ws_bytes(int set);
 size_t shared_ws_bytes(int set, bool verify, size_t batch);
 int launch_sign_shared(int set, const SignIO &io, uint8_t *ws, size_t batch, cudaStream_t st);
 int launch_verify_shared(int set, const VerifyIO &io, uint8_t *ws, size_t batch, cudaStream_t st);
+int shared_timing(int enable);
+int shared_timing_read(float *ms);
 
 }  // namespace mayo

@@ -161,6 +161,13 @@ MAYO_B200_API int mayo_b200_sign_shared(int set, const uint8_t *esk, const uint8
                                         const uint32_t *msg_len, size_t msg_stride, size_t mlen, uint8_t *sig,
                                         size_t sig_stride, uint8_t *ws, size_t batch, void *stream);
 MAYO_B200_API size_t mayo_b200_verify_shared_ws_bytes(int set, size_t batch);
+/* Profiling aid: while enabled (nonzero), each mayo_b200_sign_shared / _verify_shared call made
+ * from this host thread records CUDA events between its kernels on its stream (enable before any
+ * stream capture; it creates the events); mayo_b200_shared_timing_read waits for the last such
+ * call and gives the milliseconds of its kernels: [0] hash, [1] key tiles, [2] tensor-core
+ * product, [3] per-instance tail, [4] fix-up.  MAYO_B200_ERR_ARG if no call was recorded. */
+MAYO_B200_API int mayo_b200_shared_timing(int enable);
+MAYO_B200_API int mayo_b200_shared_timing_read(float *ms);
 MAYO_B200_API int mayo_b200_verify_shared(int set, const uint8_t *epk, const uint8_t *msgs, const uint64_t *msg_off,
                                           const uint32_t *msg_len, size_t msg_stride, size_t mlen, const uint8_t *sig,
                                           size_t sig_stride, uint8_t *result, uint8_t *ws, size_t batch,
