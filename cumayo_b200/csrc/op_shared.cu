@@ -9,8 +9,8 @@
 // so with every entry expanded to its bit matrix
 //     bit b of coordinate t of T_j[r]  =  sum over (c, b') of  Mul(P[r][c]_t)[b][b'] * bit b' of V_j[c]   (mod 2)
 // -- a 0/1 matrix A (rows (r, t, b), columns (c, b')) times a 0/1 matrix B (rows (c, b'),
-// columns (instance, j)).  The tensor cores sum the products exactly in s32 and the epilogue
-// keeps bit 0 of each sum.
+// columns (instance, j)).  A is stored as 0 / 128, so the tensor cores' exact s32 sums are
+// 128 x the integer sums and the epilogue keeps bit 7 of each.
 //
 // Kernels:
 //   shared_a_kernel     builds A from the key, tiled for the MMA (one 128-row tile = the four bit
@@ -19,8 +19,8 @@
 //   shared_gemm_kernel  one CTA per N instances' vectors (B, built in shared memory from their
 //                       nibbles, resident): for every A tile, a bulk copy (double-buffered), one
 //                       thread issues the MMAs into a TMEM accumulator (double-buffered), and eight
-//                       warps read the accumulator back (tcgen05.ld), take bit 0 of each sum with
-//                       warp ballots -- one ballot is one 32-coordinate bit plane -- and store the
+//                       warps read the accumulator back (tcgen05.ld, 16-bit halves), gather bit 7
+//                       of 32 sums into one word -- one 32-coordinate bit plane -- and store the
 //                       planes.  Zero blocks of A (columns c < r of the triangular P1 / P) are
 //                       skipped.  Waits are bounded: a timeout sets the status word and unwinds.
 //   sign: sign_hash_kernel (thread per instance) -> product -> sign_shared_tail_kernel (first
@@ -148,7 +148,7 @@ __global__ void shared_a_kernel(const uint8_t *key, uint8_t *A, uint32_t *ctl) {
             const uint32_t a = P::entry(key, rr, c, t);
             uint32_t v = 0;
 #pragma unroll
-            for (int bp = 0; bp < 4; bp++) v |= ((gf16_mul_ct(a, 1u << bp) >> b) & 1u) << (8 * bp);
+            for (int bp = 0; bp < 4; bp++) v |= ((gf16_mul_ct(a, 1u << bp) >> b) & 1u) << (8 * bp + 7);
             wd[q] = v;
         }
     }
@@ -157,16 +157,15 @@ __global__ void shared_a_kernel(const uint8_t *key, uint8_t *A, uint32_t *ctl) {
         make_uint4(wd[0], wd[1], wd[2], wd[3]);
 }
 
-// Bit 0 of 32 sums packed into one word: bit 8 j + k <- sum 4 k + j (three byte permutes per
-// four sums, then the low bits merged; the A tile's row order makes this a G4 plane).
-__device__ __forceinline__ uint32_t pack_lsb32(const uint32_t (&r)[32]) {
+// The key tiles hold 0 / 128, so every sum is 128 x (the GF(2) sum): bit 7 of its low byte is the
+// result.  The sums come from TMEM as pairs of low 16-bit halves (tcgen05.ld .pack::16b: register
+// i = sums 2i, 2i + 1 in bits 0-15, 16-31).  One permute per four sums replicates those four bit
+// 7s over bytes 0-3 (byte j <- sum 4 k + j), one LOP3 keeps bit k of each byte: bit 8 j + k <-
+// sum 4 k + j (the A tile's row order makes this a G4 plane).
+__device__ __forceinline__ uint32_t pack_bit7x32(const uint32_t (&r)[16]) {
     uint32_t x = 0;
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-        const uint32_t lo = __byte_perm(r[4 * k], r[4 * k + 1], 0x0040);
-        const uint32_t hi = __byte_perm(r[4 * k + 2], r[4 * k + 3], 0x0040);
-        x += (__byte_perm(lo, hi, 0x5410) & 0x01010101u) << k;  // disjoint bits: + is |
-    }
+    for (int k = 0; k < 8; k++) x |= tc::prmt(r[2 * k], r[2 * k + 1], 0xECA8u) & (0x01010101u << k);
     return x;
 }
 
@@ -251,10 +250,15 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
             int last_load[ST];  // last tile loaded into each stage (for the unwind)
             for (int st = 0; st < ST; st++) last_load[st] = -1;
             int consumed = -1, committed = -1;
+            // K bytes 32 s .. 32 s + 31 hold columns 8 s .. 8 s + 7; a tile's first group has
+            // the smallest row, so the smallest first nonzero column: k-steps below s0 are zero
+            // for every row of the tile and are neither copied nor multiplied
+            auto first_step = [&](int tile) { return P::c_min((tile * G) / P::W) / 8; };
             auto load = [&](int tile) {
                 const int st = tile % ST;
-                tc::mbar_arrive_expect_tx(&full[st], TILE);
-                tc::bulk_g2s(sA + (size_t)st * TILE, A + (size_t)tile * TILE, TILE, &full[st]);
+                const uint32_t skip = (uint32_t)first_step(tile) * 2u * KR * 16u;  // whole 16-byte chunks
+                tc::mbar_arrive_expect_tx(&full[st], TILE - skip);
+                tc::bulk_g2s(sA + (size_t)st * TILE + skip, A + (size_t)tile * TILE + skip, TILE - skip, &full[st]);
                 last_load[st] = tile;
             };
             for (int t = 0; t < ST && t < NT; t++) load(t);
@@ -267,9 +271,7 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
                 if (ok && i >= 2) ok = tc::mbar_wait(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, SH_SPIN);
                 if (!ok) break;
                 tc::fence_after_sync();
-                // K bytes 32 s .. 32 s + 31 hold columns 8 s .. 8 s + 7; the tile's first group has
-                // the smallest row, so the smallest first nonzero column
-                const int s0 = P::c_min((i * G) / P::W) / 8;
+                const int s0 = first_step(i);
                 for (int s = s0; s < P::KSTEPS; s++) {
                     const uint64_t kd = tc::desc_kmajor(sA_addr + (uint32_t)st * TILE + (uint32_t)s * 2u * KR * 16u,
                                                         (uint32_t)KR * 16u, 128u);
@@ -322,16 +324,16 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
                 break;
             }
             tc::fence_after_sync();
-            uint32_t r[PL][32];
+            uint32_t r[PL][16];
 #pragma unroll
-            for (int p = 0; p < PL; p++) tc::tmem_ld32(taddr + (uint32_t)b * ACC + (uint32_t)p * 32u, r[p]);
+            for (int p = 0; p < PL; p++) tc::tmem_ld32_pack16(taddr + (uint32_t)b * ACC + (uint32_t)p * 32u, r[p]);
             tc::tmem_wait_ld();
             tc::fence_before_sync();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(&acc_free[b]);  // the accumulator may be overwritten now
             uint32_t wd[PL];
 #pragma unroll
-            for (int p = 0; p < PL; p++) wd[p] = pack_lsb32(r[p]);
+            for (int p = 0; p < PL; p++) wd[p] = pack_bit7x32(r[p]);
             const int gi = i * G + g;  // group = (row gi / W, coordinate group gi % W)
             if (live && gi < P::NGROUPS) {
                 uint32_t *o = reinterpret_cast<uint32_t *>(dst + gi);
