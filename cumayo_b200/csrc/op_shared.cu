@@ -44,7 +44,9 @@ namespace mayo {
 constexpr uint32_t SH_SPIN = 1u << 22;  // mbarrier polls before a wait gives up
 constexpr size_t SH_SMEM_MAX = 226 * 1024;
 constexpr int SH_EPI_NT = 256;              // 8 epilogue warps: warp w reads TMEM lanes 32 (w % 4).., half w / 4
-constexpr int SH_GEMM_NT = SH_EPI_NT + 32;  // + one producer warp (loads, MMA issue)
+constexpr int SH_ISSUE_WARP = SH_EPI_NT / 32;       // warps 8, 9: MMA issuers (even / odd tiles)
+constexpr int SH_LOAD_WARP = SH_ISSUE_WARP + 2;     // warp 10: key loader
+constexpr int SH_GEMM_NT = SH_EPI_NT + 96;
 constexpr int SH_FIX_CTAS = 2 * 148;
 
 // The product for sign (rows: T_j[r] over P1 for r < v, then M_j[b] over L) or verify (rows
@@ -58,24 +60,30 @@ struct SharedProb {
     static constexpr int KPAD = (4 * NVEC + 31) / 32 * 32;    // bytes of one B column (K)
     static constexpr int KSTEPS = KPAD / 32;                   // MMAs of K = 32 per tile
     static constexpr int NGROUPS = NROWS * W;  // 128-row groups of the key matrix (row rr, group w)
-    // One MMA: M = 128 vector columns (NB blocks), N = KROWS = 128 G key rows (G groups per tile);
-    // an accumulator takes NB * KROWS <= 256 TMEM columns (two of them: double-buffered).  Larger
-    // MMAs first, as shared memory allows: (G 2, 128 columns), (G 1, 256 columns), (G 1, 128).
-    static constexpr size_t smem_cfg(int g, int ni, int st) {
-        return (size_t)ni * KPAD + (size_t)st * g * 128 * KPAD + 128;
-    }
-    static constexpr int G = smem_cfg(2, 128, 2) <= SH_SMEM_MAX ? 2 : 1;
-    static constexpr int NINST = G == 2 ? 128 : (smem_cfg(1, 256, 2) <= SH_SMEM_MAX ? 256 : 128);
-    static constexpr int STAGES = smem_cfg(G, NINST, 4) <= SH_SMEM_MAX   ? 4
-                                  : smem_cfg(G, NINST, 3) <= SH_SMEM_MAX ? 3
-                                  : smem_cfg(G, NINST, 2) <= SH_SMEM_MAX ? 2
-                                                                          : 1;
+    // One MMA: M = 128 vector columns, N = 128 key rows (one group), K = 32.  NB = 2 M-blocks of
+    // vectors share every k-step of key rows, so each key byte brought into shared memory feeds
+    // 256 vector columns (the key stream from L2 is what bounds this kernel); an accumulator takes
+    // NB x 128 = 256 TMEM columns (two of them: double-buffered).  The key rows stream through a
+    // ring of NCH chunks of up to CK k-steps of one tile (one bulk copy, one commit each: more
+    // frequent commits stall the tensor pipe; a chunk never spans two tiles, so its MMAs take
+    // compile-time descriptor offsets -- the single issuing thread cannot afford more than a few
+    // instructions per MMA).
+    static constexpr int G = 1;
+    static constexpr int NINST = 256;
     static constexpr int KROWS = 128 * G;
+    static constexpr size_t SLOT = (size_t)2 * KROWS * 16;  // one k-step of key rows: [2][KROWS][16 B]
+    static constexpr size_t BAR_BYTES = 1024;               // mbarriers (2 NCH + 6) and flags
+    static constexpr int nch_fit(int ck) { return (int)((SH_SMEM_MAX - (size_t)NINST * KPAD - BAR_BYTES) / (ck * SLOT)); }
+    static constexpr int CK = nch_fit(8) >= 3 ? 8 : 4;      // k-steps per chunk
+    static constexpr int NCH_FIT = nch_fit(CK);
+    static constexpr int NCH = NCH_FIT < 16 ? NCH_FIT : 16;
+    static_assert(NCH >= 2, "key ring");
+    static_assert((2 * NCH + 6) * 8 + 12 <= (int)BAR_BYTES, "barrier area");
     static constexpr int NTILES = (NGROUPS + G - 1) / G;
     static constexpr size_t TILE = (size_t)KROWS * KPAD;
     static constexpr int NB = NINST / 128;  // MMA M-blocks of 128 vector columns
     static constexpr int NI = NINST / S::k; // instances per CTA
-    static constexpr size_t SMEM = smem_cfg(G, NINST, STAGES);
+    static constexpr size_t SMEM = (size_t)NINST * KPAD + (size_t)NCH * CK * SLOT + BAR_BYTES;
     static_assert(NB * KROWS <= 256, "accumulator columns");
     static constexpr size_t PLANES = (size_t)S::k * NROWS * W;  // uint4 per instance
     // first column c that can be nonzero in row rr
@@ -176,130 +184,192 @@ __device__ __forceinline__ uint32_t pack_bit7x32(const uint32_t (&r)[16]) {
 // epilogue thread owns one vector column and reads the 32 sums of one bit plane of its tile
 // from its own TMEM lane: packing them into the plane's word is thread-local.
 //
-// Warp-specialized: warp 8 (one thread) is the producer -- it keeps STAGES key tiles in flight
-// (bulk copies), issues each tile's MMAs into one of two TMEM accumulators once that accumulator
-// has been read out, and refills a stage once the MMAs that read it completed; warps 0-7 are
-// the epilogue -- they wait for a tile's MMAs, read their sums (tcgen05.ld), hand the
-// accumulator back (acc_free), pack and store.  Barriers: full[stage] (copy landed),
-// mma_done[acc] (commit), acc_free[acc] (8 arrivals).
+// Warp-specialized: one thread of warp 10 streams the key rows (a k-step = all 128 rows of a
+// group, K = 32) through a ring of NCH chunks of up to CK k-steps of one tile, one bulk copy per
+// chunk, refilling a chunk once the MMAs that read it completed; one thread each of warps 8 and 9
+// issues the MMAs of the even / odd tiles into TMEM accumulator 0 / 1 once that accumulator has
+// been read out; warps 0-7 are the epilogue -- they wait for a tile's MMAs, read their sums
+// (tcgen05.ld), hand the accumulator back (acc_free), pack and store.  Barriers: full[chunk]
+// (copy landed), empty[chunk] (commit: its MMAs completed), mma_done[acc] (commit), acc_free[acc]
+// (8 arrivals), drain[issuer] (an issuer's last commit).  The loader starts as soon as the
+// barriers exist; the others first build the vector columns.
 template <int SET, bool VERIFY>
 __global__ void __launch_bounds__(SH_GEMM_NT, 1)
     shared_gemm_kernel(const uint8_t *__restrict__ A, const uint8_t *__restrict__ vec, size_t vec_stride,
                        uint4 *__restrict__ planes, uint32_t batch, uint32_t *ctl) {
     using P = SharedProb<SET, VERIFY>;
     using S = Set<SET>;
-    constexpr int NIN = P::NINST, KPAD = P::KPAD, NT = P::NTILES, ST = P::STAGES, NB = P::NB, G = P::G;
+    constexpr int NIN = P::NINST, KPAD = P::KPAD, NT = P::NTILES, NB = P::NB, G = P::G;
     constexpr int KR = P::KROWS;
-    constexpr uint32_t TILE = (uint32_t)P::TILE;
+    constexpr uint32_t NCH = (uint32_t)P::NCH, CK = (uint32_t)P::CK, SLOT = (uint32_t)P::SLOT;
     constexpr uint32_t IDESC = tc::idesc_u8(128, KR);
     constexpr uint32_t ACC = KR * NB;  // TMEM columns of one accumulator
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t *sB = smem;                                            // [KPAD/16][NIN][16] vector columns
-    uint8_t *sA = smem + (size_t)NIN * KPAD;                        // ST x [KPAD/16][KR][16] key tiles
-    uint64_t *full = reinterpret_cast<uint64_t *>(sA + (size_t)ST * TILE);  // [ST]
-    uint64_t *mma_done = full + ST;                                 // [2]
+    uint8_t *ring = smem + (size_t)NIN * KPAD;                      // NCH x CK x [2][KR][16] key rows
+    uint64_t *full = reinterpret_cast<uint64_t *>(ring + (size_t)NCH * CK * SLOT);  // [NCH]
+    uint64_t *empty = full + NCH;                                   // [NCH]
+    uint64_t *mma_done = empty + NCH;                               // [2]
     uint64_t *acc_free = mma_done + 2;                              // [2]
-    uint32_t *s_tmem = reinterpret_cast<uint32_t *>(acc_free + 2);
+    uint64_t *drain = acc_free + 2;                                 // [2]
+    uint32_t *s_tmem = reinterpret_cast<uint32_t *>(drain + 2);
     uint32_t *s_fail = s_tmem + 1;
+    uint32_t *s_loaded = s_tmem + 2;  // chunks whose copy the loader has started (armed full[])
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t inst0 = blockIdx.x * (uint32_t)P::NI;
 
     if (tid == 0) {
-        for (int i = 0; i < ST; i++) tc::mbar_init(&full[i], 1);
+        for (uint32_t i = 0; i < NCH; i++) {
+            tc::mbar_init(&full[i], 1);
+            tc::mbar_init(&empty[i], 1);
+        }
         for (int i = 0; i < 2; i++) {
             tc::mbar_init(&mma_done[i], 1);
             tc::mbar_init(&acc_free[i], SH_EPI_NT / 32);
         }
+        tc::mbar_init(&drain[0], 1);
+        tc::mbar_init(&drain[1], 1);
         tc::fence_mbar_init();
         *s_fail = 0;
+        *s_loaded = 0;
     }
     if (warp == 0) {
         tc::tmem_alloc(s_tmem, 2 * ACC);
         tc::tmem_relinquish();
     }
-    // vector columns: column n = (instance n / k, vector j = n % k); K byte 4 c + b' = bit b' of entry c
-    for (int idx = tid; idx < (KPAD / 16) * NIN; idx += SH_GEMM_NT) {
-        const int ch = idx / NIN, n = idx - ch * NIN;
-        const uint32_t inst = inst0 + (uint32_t)(n / S::k);
-        const int j = n % S::k;
-        uint32_t wd[4] = {0u, 0u, 0u, 0u};
-        if (n < P::NI * S::k && inst < batch) {
-            const uint8_t *vp = vec + (size_t)inst * vec_stride;
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int c = 4 * ch + q;
-                if (c < P::NVEC) {
-                    const int nib = j * P::NVEC + c;
-                    const uint32_t x = (vp[nib >> 1] >> ((nib & 1) * 4)) & 0xFu;
-                    wd[q] = (x * 0x00204081u) & 0x01010101u;  // bit b' -> byte b'
-                }
-            }
-        }
-        *reinterpret_cast<uint4 *>(sB + ((size_t)ch * NIN + n) * 16) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
-    }
-    tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tbase = *s_tmem;
-
-    if (warp == SH_EPI_NT / 32) {
-        // ---------------- producer ----------------
+    // K bytes 32 s .. 32 s + 31 hold columns 8 s .. 8 s + 7; a tile's first group has the smallest
+    // row, so the smallest first nonzero column: k-steps below s0 are zero for every row of the
+    // tile and are neither copied nor multiplied
+    auto first_step = [](int tile) { return P::c_min((tile * G) / P::W) / 8; };
+    // Every CTA walks all tiles, starting at its own offset: CTAs that run at the same time then
+    // read different key rows, spread over the L2 slices.  The i-th tile of this CTA is tile_of(i).
+    const int t_off = (int)((blockIdx.x % 128u) * (uint32_t)NT / 128u);
+    auto tile_of = [&](int i) { return i + t_off < NT ? i + t_off : i + t_off - NT; };
+    if (warp == SH_LOAD_WARP) {
+        // ---------------- loader: chunk c (k-steps a .. a + n - 1 of one tile) -> slot c % NCH ----------------
         if (lane == 0) {
-            const uint32_t sA_addr = tc::smem_u32(sA), sB_addr = tc::smem_u32(sB);
-            int last_load[ST];  // last tile loaded into each stage (for the unwind)
-            for (int st = 0; st < ST; st++) last_load[st] = -1;
-            int consumed = -1, committed = -1;
-            // K bytes 32 s .. 32 s + 31 hold columns 8 s .. 8 s + 7; a tile's first group has
-            // the smallest row, so the smallest first nonzero column: k-steps below s0 are zero
-            // for every row of the tile and are neither copied nor multiplied
-            auto first_step = [&](int tile) { return P::c_min((tile * G) / P::W) / 8; };
-            auto load = [&](int tile) {
-                const int st = tile % ST;
-                const uint32_t skip = (uint32_t)first_step(tile) * 2u * KR * 16u;  // whole 16-byte chunks
-                tc::mbar_arrive_expect_tx(&full[st], TILE - skip);
-                tc::bulk_g2s(sA + (size_t)st * TILE + skip, A + (size_t)tile * TILE + skip, TILE - skip, &full[st]);
-                last_load[st] = tile;
-            };
-            for (int t = 0; t < ST && t < NT; t++) load(t);
+            uint32_t c = 0;
             bool ok = true;
 #pragma unroll 1
             for (int i = 0; i < NT && ok; i++) {
-                const int st = i % ST, b = i & 1;
-                ok = tc::mbar_wait(&full[st], (uint32_t)(i / ST) & 1u, SH_SPIN);
-                if (ok) consumed = i;
-                if (ok && i >= 2) ok = tc::mbar_wait(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, SH_SPIN);
-                if (!ok) break;
-                tc::fence_after_sync();
-                const int s0 = first_step(i);
-                for (int s = s0; s < P::KSTEPS; s++) {
-                    const uint64_t kd = tc::desc_kmajor(sA_addr + (uint32_t)st * TILE + (uint32_t)s * 2u * KR * 16u,
-                                                        (uint32_t)KR * 16u, 128u);
-#pragma unroll
-                    for (int h = 0; h < NB; h++) {
-                        const uint64_t vd = tc::desc_kmajor(sB_addr + (uint32_t)s * 2u * NIN * 16u + (uint32_t)h * 2048u,
-                                                            (uint32_t)NIN * 16u, 128u);
-                        tc::mma_i8(tbase + (uint32_t)b * ACC + (uint32_t)h * KR, vd, kd, IDESC, s > s0 ? 1u : 0u);
+                const int t = tile_of(i);
+                const uint8_t *src = A + (size_t)t * P::TILE;
+#pragma unroll 1
+                for (int a = first_step(t); a < P::KSTEPS; a += (int)CK, c++) {
+                    const uint32_t cs = c % NCH;
+                    if (*reinterpret_cast<volatile uint32_t *>(s_fail) ||
+                        (c >= NCH && !tc::mbar_wait(&empty[cs], (c / NCH - 1) & 1u, SH_SPIN))) {
+                        ok = false;
+                        break;
                     }
+                    const uint32_t n = P::KSTEPS - a < (int)CK ? (uint32_t)(P::KSTEPS - a) : CK;
+                    tc::mbar_arrive_expect_tx(&full[cs], n * SLOT);
+                    tc::bulk_g2s(ring + (size_t)cs * CK * SLOT, src + (size_t)a * SLOT, n * SLOT, &full[cs]);
+                    __threadfence_block();
+                    *reinterpret_cast<volatile uint32_t *>(s_loaded) = c + 1;
                 }
-                tc::mma_commit(&mma_done[b]);
-                committed = i;
-                // refill: with several stages, the stage of tile i - 1 (free once its MMAs
-                // completed, while tile i's run); with one stage, tile i's own after its MMAs
-                constexpr int D = ST > 1 ? 1 : 0;
-                if (i >= D && i - D + ST < NT) {
-                    ok = tc::mbar_wait(&mma_done[(i - D) & 1], (uint32_t)((i - D) >> 1) & 1u, SH_SPIN);
-                    if (ok) load(i - D + ST);
-                }
-                if (*reinterpret_cast<volatile uint32_t *>(s_fail)) ok = false;
             }
             if (!ok) atomicOr(s_fail, 1u);
-            // unwind: no copy or MMA of this CTA may be in flight when TMEM is freed
-            for (int st = 0; st < ST; st++)
-                if (last_load[st] > consumed) tc::mbar_wait(&full[st], (uint32_t)(last_load[st] / ST) & 1u, SH_SPIN);
-            if (committed >= 0) tc::mbar_wait(&mma_done[committed & 1], (uint32_t)(committed >> 1) & 1u, SH_SPIN);
+            // unwind: no copy of this CTA may be in flight when it exits (the last chunk loaded
+            // into each slot is the latest phase of its barrier)
+            for (uint32_t ch = c > NCH ? c - NCH : 0; ch < c; ch++)
+                tc::mbar_wait(&full[ch % NCH], (ch / NCH) & 1u, SH_SPIN);
         }
     } else {
+        // vector columns: column n = (instance n / k, vector j = n % k); K byte 4 c + b' = bit b' of entry c
+        for (int idx = tid; idx < (KPAD / 16) * NIN; idx += SH_LOAD_WARP * 32) {
+            const int ch = idx / NIN, n = idx - ch * NIN;
+            const uint32_t inst = inst0 + (uint32_t)(n / S::k);
+            const int j = n % S::k;
+            uint32_t wd[4] = {0u, 0u, 0u, 0u};
+            if (n < P::NI * S::k && inst < batch) {
+                const uint8_t *vp = vec + (size_t)inst * vec_stride;
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int c = 4 * ch + q;
+                    if (c < P::NVEC) {
+                        const int nib = j * P::NVEC + c;
+                        const uint32_t x = (vp[nib >> 1] >> ((nib & 1) * 4)) & 0xFu;
+                        wd[q] = (x * 0x00204081u) & 0x01010101u;  // bit b' -> byte b'
+                    }
+                }
+            }
+            *reinterpret_cast<uint4 *>(sB + ((size_t)ch * NIN + n) * 16) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+        }
+        tc::fence_async_smem();
+        bar_sync(1, SH_LOAD_WARP * 32);  // warps 0-9: the vector columns are in place
+    }
+    if (warp == SH_ISSUE_WARP || warp == SH_ISSUE_WARP + 1) {
+        // ---------------- MMA issuers: warp 8 the even tiles, warp 9 the odd ones ----------------
+        // Two issuers, so one issues while the other waits and does its bookkeeping: tiles are
+        // only 5-20 k-steps, and a single thread's per-tile overhead left the tensor pipe idle.
+        const int me = warp - SH_ISSUE_WARP;
+        if (lane == 0) {
+            const uint64_t kd0 = tc::desc_kmajor(tc::smem_u32(ring), (uint32_t)KR * 16u, 128u);
+            const uint64_t vd0 = tc::desc_kmajor(tc::smem_u32(sB), (uint32_t)NIN * 16u, 128u);
+            // descriptor start addresses are in 16-byte units (bits 0-13; every address here is
+            // below 2^18 bytes, so adding to the descriptor never carries out of the field)
+            constexpr uint64_t KD_STEP = SLOT >> 4, VD_STEP = (2u * NIN * 16u) >> 4, VD_BLOCK = 2048u >> 4;
+            uint32_t c = 0;  // global chunk number (the loader's order)
+            bool ok = true;
+#pragma unroll 1
+            for (int i = 0; i < NT && ok; i++) {
+                const int s0 = first_step(tile_of(i));
+                if ((i & 1) != me) {  // the other issuer's tile: skip its chunks
+                    c += (uint32_t)((P::KSTEPS - s0 + (int)CK - 1) / (int)CK);
+                    continue;
+                }
+                const int b = i & 1;
+                if (i >= 2 && !tc::mbar_wait(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, SH_SPIN)) {
+                    ok = false;
+                    break;
+                }
+                tc::fence_after_sync();
+                const uint32_t dacc = tbase + (uint32_t)b * ACC;
+#pragma unroll 1
+                for (int a = s0; a < P::KSTEPS; a += (int)CK, c++) {
+                    const uint32_t cs = c % NCH;
+                    // The other issuer's tile may hold unloaded chunks older than c, so slot cs
+                    // can still be a phase behind chunk c: a parity wait is only meaningful once
+                    // the loader has armed chunk c's phase.
+                    uint32_t spin = 0;
+                    while (*reinterpret_cast<volatile uint32_t *>(s_loaded) <= c && ++spin < SH_SPIN) {
+                    }
+                    __threadfence_block();
+                    if (spin >= SH_SPIN || !tc::mbar_wait(&full[cs], (c / NCH) & 1u, SH_SPIN)) {
+                        ok = false;
+                        break;
+                    }
+                    const int n = P::KSTEPS - a;  // k-steps of this chunk: min(n, CK)
+                    const uint64_t kdc = kd0 + (uint64_t)cs * (CK * KD_STEP);
+                    const uint64_t vdc = vd0 + (uint64_t)a * VD_STEP;
+                    const uint32_t acc0 = a > s0 ? 1u : 0u;
+#pragma unroll
+                    for (int u = 0; u < (int)CK; u++) {
+                        if (u < n) {
+#pragma unroll
+                            for (int h = 0; h < NB; h++)
+                                tc::mma_i8(dacc + (uint32_t)h * KR, vdc + (uint64_t)u * VD_STEP + (uint64_t)h * VD_BLOCK,
+                                           kdc + (uint64_t)u * KD_STEP, IDESC, u > 0 ? 1u : acc0);
+                        }
+                    }
+                    tc::mma_commit(&empty[cs]);  // the chunk may be refilled once these MMAs completed
+                }
+                if (!ok) break;
+                tc::mma_commit(&mma_done[b]);  // the accumulator may be read
+                if ((i & 15) == me && *reinterpret_cast<volatile uint32_t *>(s_fail)) ok = false;
+            }
+            if (!ok) atomicOr(s_fail, 1u);
+            // unwind: every MMA of this thread (and so every commit arrival it issued before)
+            // lands before TMEM is freed
+            tc::mma_commit(&drain[me]);
+            tc::mbar_wait(&drain[me], 0u, SH_SPIN);
+        }
+    } else if (warp < SH_ISSUE_WARP) {
         // ---------------- epilogue ----------------
         // warp: TMEM lanes 32 (warp % 4).. = vector columns.  Warps 0-3 / 4-7 split the work:
         // two M-blocks -> block 0 / 1, all four planes; two groups per tile -> group 0 / 1;
@@ -334,7 +404,7 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
             uint32_t wd[PL];
 #pragma unroll
             for (int p = 0; p < PL; p++) wd[p] = pack_bit7x32(r[p]);
-            const int gi = i * G + g;  // group = (row gi / W, coordinate group gi % W)
+            const int gi = tile_of(i) * G + g;  // group = (row gi / W, coordinate group gi % W)
             if (live && gi < P::NGROUPS) {
                 uint32_t *o = reinterpret_cast<uint32_t *>(dst + gi);
                 if (PL == 4)

@@ -82,3 +82,40 @@ def test_shared_key_sign_verify_match(cuda, s):
         assert int(vws[:4].cpu().numpy().view(np.uint32)[0]) == 0, "tensor-core product fell back"
         assert res.cpu().numpy().tolist() == bad.astype(np.uint8).tolist()
         assert torch.equal(res, res_ref)
+
+
+@pytest.mark.parametrize("s", [1, 2, 3, 5])
+def test_shared_key_large_batch(cuda, s):
+    """Thousands of instances: every SM runs product CTAs at once, so the key stream from L2 lags
+    the tensor cores and the loader / issuer / epilogue handshakes are exercised under load."""
+    import torch
+    m = Mayo(s)
+    z = m.sizes
+    n = 8192 if s == 2 else 4096
+    mlen = 32
+    sk, pk = O.keypair(s, 1, 0)
+    esk = _dev(np.frombuffer(O.expandsk(s, sk), np.uint8))
+    epk = _dev(np.frombuffer(O.expandpk(s, pk), np.uint8))
+    rng = np.random.default_rng(7 + s)
+    d_msg = _dev(rng.integers(0, 256, n * mlen, dtype=np.uint8))
+    sig_ref = torch.zeros(n * z.sig_bytes, dtype=torch.uint8, device="cuda")
+    ws_ref = torch.zeros(n * m.sign_ws_bytes(), dtype=torch.uint8, device="cuda")
+    m.sign_many(esk, d_msg, sig_ref, ws_ref, n, msg_stride=mlen, mlen=mlen)
+    ws = torch.zeros(max(m.sign_shared_ws_bytes(n), m.verify_shared_ws_bytes(n)), dtype=torch.uint8, device="cuda")
+    sig = torch.zeros(n * z.sig_bytes, dtype=torch.uint8, device="cuda")
+    m.sign_shared(esk, d_msg, sig, ws, n, msg_stride=mlen, mlen=mlen)
+    torch.cuda.synchronize()
+    assert int(ws[:4].cpu().numpy().view(np.uint32)[0]) == 0, "tensor-core product fell back"
+    assert torch.equal(sig, sig_ref)
+    vsig = sig.clone().view(n, z.sig_bytes)
+    vsig[::7, 3] ^= 0x10
+    res_ref = torch.full((n,), 0xEE, dtype=torch.uint8, device="cuda")
+    m.verify_many(epk, d_msg, vsig.view(-1), res_ref, n, msg_stride=mlen, mlen=mlen)
+    res = torch.full((n,), 0xEE, dtype=torch.uint8, device="cuda")
+    m.verify_shared(epk, d_msg, vsig.view(-1), res, ws, n, msg_stride=mlen, mlen=mlen)
+    torch.cuda.synchronize()
+    assert int(ws[:4].cpu().numpy().view(np.uint32)[0]) == 0, "tensor-core product fell back"
+    assert torch.equal(res, res_ref)
+    expect = np.zeros(n, np.uint8)
+    expect[::7] = 1
+    assert res.cpu().numpy().tolist() == expect.tolist()
