@@ -510,8 +510,12 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
     for (int q = 0; q < CPT; q++)
         if (KO - (tid + NT * q) == 0) publish(q, 0);
     __syncthreads();
+    // Warp w owns columns <= KO - 32 w, so after step KO - 32 w - 1 it has nothing left to update
+    // or publish: it leaves the loop, and the steps' barrier counts only the warps still in it
+    // (the lowest ones; a public function of the step).
+    const int last_step = KO - 32 * (tid >> 5) - 1;
 #pragma unroll 1
-    for (int pc = 0; pc < KO; pc++) {
+    for (int pc = 0; pc <= last_step; pc++) {
         // Every column right of pc: col ^= col[p] * F'  (eliminates row p elsewhere, normalises
         // row p).  A column left of pc is already a unit vector e_p' (or has no entry in an
         // unpivoted row), so col[p] = 0 there for every later pivot row p and the update would
@@ -546,13 +550,17 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
             for (int w = 0; w < W; w++) g4_madd(col[q][w], F[w], em);
             if (c == pc + 1 && c < KO) publish(q, c);
         }
-        __syncthreads();
+        const int nw = (KO - 1 - pc) / 32 + 1;  // warps with a column > pc (or column pc + 1)
+        bar_sync(1, 32 * (nw < NT / 32 ? nw : NT / 32));
     }
-    // rank test (sign.cu:107-115 rejects when the last echelon row is zero, i.e. rank < m)
-    int rank = 0;
+    // rank test (sign.cu:107-115 rejects when the last echelon row is zero, i.e. rank < m): thread
+    // 0 took part in every step, so its record of the pivot rows is complete
+    if (tid == 0) {
+        int rank = 0;
 #pragma unroll
-    for (int w = 0; w < W; w++) rank += __popc(pivoted[w]);
-    const bool ok = rank == S::m;
+        for (int w = 0; w < W; w++) rank += __popc(pivoted[w]);
+        s_flag[0] = rank == S::m ? 1 : 0;
+    }
     // publish the reduced RHS; x = r + z (z_c = rhs[p(c)] on pivot columns)
 #pragma unroll
     for (int q = 0; q < CPT; q++)
@@ -560,6 +568,7 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
 #pragma unroll
             for (int w = 0; w < W; w++) g4_st(rhsacc + w, col[q][w]);  // not a buffer still being read
     __syncthreads();
+    const bool ok = s_flag[0] != 0;
 #pragma unroll
     for (int q = 0; q < CPT; q++) {
         const int c = KO - (tid + NT * q);
@@ -579,9 +588,8 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
             s_x[c] = (uint8_t)(rr[q] ^ (ok ? z : 0u));
         }
     }
-    if (tid == 0) s_flag[0] = ok ? 1 : 0;
     __syncthreads();
-    return s_flag[0] != 0;
+    return ok;
 }
 
 // s = V + O x, then salt (sign.cu:147-191, 474-477).
