@@ -112,7 +112,7 @@ struct SharedProb {
 };
 
 // Workspace: control words ([0] status: 0 = product ran, 1 = it gave up; [1] sign retries), A
-// tiles, per-instance hash results (sign: digest, salt, t, V || r; verify: t), per-instance
+// tiles, (sign) the O planes of the key, per-instance hash results (sign: digest, salt, t, V || r; verify: t), per-instance
 // planes, (sign) the list of instances whose first attempt was singular.
 template <int SET, bool VERIFY>
 struct SharedWs {
@@ -120,28 +120,40 @@ struct SharedWs {
     static constexpr int NW = (Set<SET>::menc + 3) / 4;
     static constexpr size_t a = 256;
     static constexpr size_t a_bytes = (size_t)P::NTILES * P::TILE;
+    static constexpr int OPL = VERIFY ? 0 : Set<SET>::o * Set<SET>::W;  // O planes (sign), uint4 items
+    static constexpr size_t op_bytes = (size_t)OPL * 16;
     static constexpr size_t inst = VERIFY ? pad16((size_t)NW * 4) : pad16(SignWs<SET>::total);
     static constexpr size_t planes = P::PLANES * 16;
     static constexpr size_t retry = VERIFY ? 0 : 4;
-    static size_t bytes(size_t batch) { return a + a_bytes + batch * (inst + planes + retry); }
-    static size_t inst_off() { return a + a_bytes; }
-    static size_t planes_off(size_t batch) { return a + a_bytes + batch * inst; }
-    static size_t retry_off(size_t batch) { return a + a_bytes + batch * (inst + planes); }
+    static constexpr size_t head = a + a_bytes + op_bytes;
+    static size_t bytes(size_t batch) { return head + batch * (inst + planes + retry); }
+    static size_t op_off() { return a + a_bytes; }
+    static size_t inst_off() { return head; }
+    static size_t planes_off(size_t batch) { return head + batch * inst; }
+    static size_t retry_off(size_t batch) { return head + batch * (inst + planes); }
 };
 
 // A, tiled: group gi = rr * W + w holds rows rho = 32 b + q (bit plane b; row q carries coordinate
 // 32 w + cq(q), cq(q) = 8 ((q >> 2) & 3) + 2 (q & 3) + (q >> 4), the order in which the epilogue's
 // packing of 32 sums lands each coordinate on its bit of a G4 plane) and K bytes 4 c + b'; a
 // tile is G consecutive groups, layout [K / 16][G * 128 rows][16 bytes].  One thread per 16
-// bytes.  Also resets the control words.
+// bytes.  Also resets the control words and (sign) writes the key's O planes after the tiles,
+// one thread per item.
 template <int SET, bool VERIFY>
-__global__ void shared_a_kernel(const uint8_t *key, uint8_t *A, uint32_t *ctl) {
+__global__ void shared_a_kernel(const uint8_t *key, uint8_t *A, uint32_t *ctl, uint4 *opl) {
     using P = SharedProb<SET, VERIFY>;
     using S = Set<SET>;
     constexpr size_t per_group = (size_t)(P::KPAD / 16) * 128;
+    constexpr size_t a_items = (size_t)P::NTILES * P::G * per_group;
     const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx < 2) ctl[idx] = 0;
-    if (idx >= (size_t)P::NTILES * P::G * per_group) return;
+    if (idx >= a_items) {
+        if constexpr (!VERIFY) {  // key = esk = seed_sk || O || P1 || L
+            if (idx < a_items + (size_t)SharedWs<SET, false>::OPL)
+                g4_st(opl + (idx - a_items), o_plane_item<SET>(key + S::sk, (int)(idx - a_items)));
+        }
+        return;
+    }
     const int gi = (int)(idx / per_group);  // group (the last tile's second group may be padding)
     const int rem = (int)(idx - (size_t)gi * per_group);
     const int ch = rem / 128, rho = rem - ch * 128;
@@ -430,7 +442,7 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
 template <int SET>
 __global__ void __launch_bounds__(SignCfg<SET>::NT)
     sign_shared_tail_kernel(const uint8_t *esk, uint8_t *sig, size_t sig_stride, const uint8_t *wsi, size_t wsi_stride,
-                            const uint4 *planes, uint32_t *ctl, uint32_t *retry) {
+                            const uint4 *planes, const uint4 *opl, uint32_t *ctl, uint32_t *retry) {
     using P = SharedProb<SET, false>;
     extern __shared__ __align__(16) uint8_t smem[];
     constexpr int NT = SignCfg<SET>::NT;
@@ -439,7 +451,7 @@ __global__ void __launch_bounds__(SignCfg<SET>::NT)
     const uint32_t inst = blockIdx.x;
     sign_load_ws<SET, NT, true>(smem, tid, esk, wsi + (size_t)inst * wsi_stride);
     if (sign_attempt<SET, NT, true>(smem, tid, esk, planes + (size_t)inst * P::PLANES)) {
-        sign_write<SET, NT, true>(smem, tid, esk, sig + (size_t)inst * sig_stride);
+        sign_write<SET, NT, true>(smem, tid, esk, sig + (size_t)inst * sig_stride, opl);
     } else if (tid == 0) {
         retry[atomicAdd(&ctl[1], 1u)] = inst;
     }
@@ -450,7 +462,7 @@ __global__ void __launch_bounds__(SignCfg<SET>::NT)
 template <int SET>
 __global__ void __launch_bounds__(SignCfg<SET>::NT)
     sign_shared_fix_kernel(const uint8_t *esk, uint8_t *sig, size_t sig_stride, const uint8_t *wsi, size_t wsi_stride,
-                           const uint32_t *ctl, const uint32_t *retry, uint32_t batch) {
+                           const uint4 *opl, const uint32_t *ctl, const uint32_t *retry, uint32_t batch) {
     extern __shared__ __align__(16) uint8_t smem[];
     constexpr int NT = SignCfg<SET>::NT;
     const int tid = threadIdx.x;
@@ -465,7 +477,7 @@ __global__ void __launch_bounds__(SignCfg<SET>::NT)
             if (ctr > 0) sign_next_vr<SET, NT>(smem, tid, ctr);
             if (sign_attempt<SET, NT>(smem, tid, esk)) break;
         }
-        sign_write<SET, NT>(smem, tid, esk, sig + (size_t)inst * sig_stride);
+        sign_write<SET, NT>(smem, tid, esk, sig + (size_t)inst * sig_stride, opl);
         __syncthreads();
     }
 }
@@ -616,8 +628,9 @@ static int launch_product(const uint8_t *key, const uint8_t *vec, size_t vec_str
     using WSL = SharedWs<SET, VERIFY>;
     uint32_t *ctl = reinterpret_cast<uint32_t *>(ws);
     uint8_t *A = ws + WSL::a;
-    const size_t a_threads = (size_t)P::NTILES * P::G * (P::KPAD / 16) * 128;
-    shared_a_kernel<SET, VERIFY><<<(unsigned)((a_threads + 255) / 256), 256, 0, st>>>(key, A, ctl);
+    const size_t a_threads = (size_t)P::NTILES * P::G * (P::KPAD / 16) * 128 + WSL::OPL;
+    shared_a_kernel<SET, VERIFY><<<(unsigned)((a_threads + 255) / 256), 256, 0, st>>>(
+        key, A, ctl, reinterpret_cast<uint4 *>(ws + WSL::op_off()));
     tmark(st);
     if (!set_smem_attr(shared_gemm_kernel<SET, VERIFY>, P::SMEM)) return ST_CUDA;
     uint4 *planes = reinterpret_cast<uint4 *>(ws + WSL::planes_off(batch));
@@ -650,11 +663,12 @@ static int sign_shared_t(const SignIO &io0, uint8_t *ws, size_t batch, cudaStrea
     if (!set_smem_attr(sign_shared_tail_kernel<SET>, CT::total)) return ST_CUDA;
     sign_shared_tail_kernel<SET><<<(unsigned)batch, CT::NT, CT::total, st>>>(
         io.esk, io.sig, io.sig_stride, io.ws, io.ws_stride, reinterpret_cast<const uint4 *>(ws + WSL::planes_off(batch)),
-        ctl, retry);
+        reinterpret_cast<const uint4 *>(ws + WSL::op_off()), ctl, retry);
     tmark(st);
     if (!set_smem_attr(sign_shared_fix_kernel<SET>, CF::total)) return ST_CUDA;
-    sign_shared_fix_kernel<SET><<<fix_grid(batch), CF::NT, CF::total, st>>>(io.esk, io.sig, io.sig_stride, io.ws,
-                                                                            io.ws_stride, ctl, retry, (uint32_t)batch);
+    sign_shared_fix_kernel<SET><<<fix_grid(batch), CF::NT, CF::total, st>>>(
+        io.esk, io.sig, io.sig_stride, io.ws, io.ws_stride, reinterpret_cast<const uint4 *>(ws + WSL::op_off()), ctl,
+        retry, (uint32_t)batch);
     tmark(st);
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
 }

@@ -592,9 +592,31 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
     return ok;
 }
 
-// s = V + O x, then salt (sign.cu:147-191, 474-477).
+// Column q of O as bit planes, coordinate group w (item q * W + w): O is row-major v x o nibbles
+// (O[t][q] at nibble t * o + q of the O block of esk).  A property of the key alone, so the
+// shared-key path computes it once per call.
+template <int SET>
+__device__ __forceinline__ G4 o_plane_item(const uint8_t *O_g, int idx) {
+    using S = Set<SET>;
+    constexpr int W = S::W;
+    const int q = idx / W, w = idx - q * W;
+    uint32_t pk[4] = {0u, 0u, 0u, 0u};
+#pragma unroll 4
+    for (int e = 0; e < 32; e++) {
+        const int t = 32 * w + e;
+        if (t < S::m) {
+            const int oi = t * S::o + q;
+            pk[e >> 3] |= (uint32_t)((O_g[oi >> 1] >> ((oi & 1) * 4)) & 0xF) << (4 * (e & 7));
+        }
+    }
+    return g4_from_packed(pk[0], pk[1], pk[2], pk[3]);
+}
+
+// s = V + O x, then salt (sign.cu:147-191, 474-477).  `opl`, when given, holds the O planes
+// (o x W items of o_plane_item) precomputed for the key.
 template <int SET, int NT_, bool CP_ = false>
-__device__ __forceinline__ void sign_write(uint8_t *smem, int tid, const uint8_t *esk, uint8_t *sig) {
+__device__ __forceinline__ void sign_write(uint8_t *smem, int tid, const uint8_t *esk, uint8_t *sig,
+                                           const uint4 *opl = nullptr) {
     MAYO_SIGN_VIEWS
     uint4 *masks = reinterpret_cast<uint4 *>(smem + C::off_masks);
     uint4 *bs = reinterpret_cast<uint4 *>(smem + C::off_bs);
@@ -611,33 +633,27 @@ __device__ __forceinline__ void sign_write(uint8_t *smem, int tid, const uint8_t
     uint8_t *s_x = smem + C::off_xs;
     int *s_flag = reinterpret_cast<int *>(smem + C::off_flag);
     (void)masks; (void)bs; (void)acol; (void)xacc; (void)upk; (void)mpk; (void)pivbuf; (void)rhsacc; (void)ypk; (void)s_key; (void)s_t; (void)s_vr; (void)s_x; (void)s_flag;
-    // s_i = V_i + O x_i on bit planes: the columns of O as planes (the engine staging area, free
-    // after the attempt), then per (i, group w) o multiply-accumulates; nibbles staged one per
-    // byte (the mask area, also free) because s_i starts mid-byte when n is odd.
-    const uint8_t *O_g = esk + S::sk;
+    // s_i = V_i + O x_i on bit planes: the columns of O as planes and the k x W accumulators in
+    // the engine staging area (free after the attempt); each accumulator (i, w) takes its o
+    // multiply-accumulates from SPL threads (shared-memory XOR to combine); nibbles are staged
+    // one per byte (the mask area, also free) because s_i starts mid-byte when n is odd.
+    constexpr int SPL = 4;
     uint4 *ocol = reinterpret_cast<uint4 *>(smem + C::off_bs);  // [o][W]
+    uint4 *sacc = ocol + S::o * W;                                 // [k][W]
     uint8_t *snib = smem + C::off_masks;                           // [k * n]
-    static_assert((size_t)S::o * W * 16 <= (C::sz_bs > C::sz_acol ? C::sz_bs : C::sz_acol), "O planes fit");
+    static_assert((size_t)(S::o + S::k) * W * 16 <= (C::sz_bs > C::sz_acol ? C::sz_bs : C::sz_acol),
+                  "O planes and s accumulators fit");
     static_assert((size_t)S::k * S::n <= (size_t)S::v * J * 16, "nibble staging fits");
-    for (int idx = tid; idx < S::o * W; idx += NT) {
-        const int q = idx / W, w = idx - q * W;
-        uint32_t pk[4] = {0u, 0u, 0u, 0u};
-#pragma unroll 4
-        for (int e = 0; e < 32; e++) {
-            const int t = 32 * w + e;
-            if (t < S::m) {
-                const int oi = t * S::o + q;
-                pk[e >> 3] |= (uint32_t)((O_g[oi >> 1] >> ((oi & 1) * 4)) & 0xF) << (4 * (e & 7));
-            }
-        }
-        g4_st(ocol + idx, g4_from_packed(pk[0], pk[1], pk[2], pk[3]));
+    if (opl) {
+        for (int idx = tid; idx < S::o * W; idx += NT) ocol[idx] = opl[idx];
+    } else {
+        for (int idx = tid; idx < S::o * W; idx += NT) g4_st(ocol + idx, o_plane_item<SET>(esk + S::sk, idx));
     }
     for (int idx = tid; idx < S::k * S::o; idx += NT) {  // x_i: the last o nibbles of s_i
         const int i = idx / S::o, q = idx - i * S::o;
         snib[i * S::n + S::m + q] = s_x[idx];
     }
-    __syncthreads();
-    for (int idx = tid; idx < S::k * W; idx += NT) {
+    for (int idx = tid; idx < S::k * W; idx += NT) {  // accumulator (i, w) starts as V_i group w
         const int i = idx / W, w = idx - i * W;
         // V_i group w: packed nibbles i * m + 32 w .. (m even, so byte aligned)
         const uint8_t *vb = s_vr + (i * S::m + 32 * w) / 2;
@@ -648,13 +664,28 @@ __device__ __forceinline__ void sign_write(uint8_t *smem, int tid, const uint8_t
             const int last = S::m - 32 * w;
             pk[last >> 3] &= ~(0xFu << (4 * (last & 7)));
         }
-        G4 acc = g4_from_packed(pk[0], pk[1], pk[2], pk[3]);
+        g4_st(sacc + idx, g4_from_packed(pk[0], pk[1], pk[2], pk[3]));
+    }
+    __syncthreads();
+    for (int idx = tid; idx < S::k * W * SPL; idx += NT) {
+        const int g = idx / SPL, part = idx - g * SPL;
+        const int i = g / W, w = g - i * W;
+        G4 acc = g4_zero();
 #pragma unroll 1
-        for (int q = 0; q < S::o; q++) g4_madd(acc, g4_ld(ocol + q * W + w), scalar_masks(s_x[i * S::o + q]));
-        const uint4 u = g4_to_packed(acc);
-        const uint32_t wd[4] = {u.x, u.y, u.z, u.w};
-        for (int e = 0; e < 32 && 32 * w + e < S::m; e++)
-            snib[i * S::n + 32 * w + e] = (uint8_t)((wd[e >> 3] >> (4 * (e & 7))) & 0xF);
+        for (int q = part; q < S::o; q += SPL) g4_madd(acc, g4_ld(ocol + q * W + w), scalar_masks(s_x[i * S::o + q]));
+        g4_atomic_xor(sacc + g, acc);
+    }
+    __syncthreads();
+    for (int idx = tid; idx < S::k * W * 4; idx += NT) {  // packed word qw of accumulator (i, w) -> 8 nibbles
+        const int g = idx >> 2, qw = idx & 3;
+        const int i = g / W, w = g - i * W;
+        const uint4 u = g4_to_packed(g4_ld(sacc + g));
+        const uint32_t wd = qw == 0 ? u.x : (qw == 1 ? u.y : (qw == 2 ? u.z : u.w));
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const int c = 32 * w + 8 * qw + e;
+            if (c < S::m) snib[i * S::n + c] = (uint8_t)((wd >> (4 * e)) & 0xF);
+        }
     }
     __syncthreads();
     uint8_t *sigp = sig;
