@@ -420,6 +420,26 @@ __host__ __device__ constexpr uint64_t gf16_inv_table() {
     return t;
 }
 constexpr uint64_t kGf16InvTable = gf16_inv_table();
+// Division table: byte 16 p + e = e / p (e times the inverse of p; row p = 0 all zero), four bytes
+// per word, little-endian.
+struct Gf16DivTable {
+    uint32_t w[64];
+};
+__host__ __device__ constexpr Gf16DivTable gf16_div_table() {
+    Gf16DivTable t{};
+    for (uint32_t p = 0; p < 16; p++) {
+        uint32_t inv = 0;
+        for (uint32_t b = 1; b < 16; b++)
+            if (gf16_mul_cx(p, b) == 1) inv = b;
+        for (uint32_t e = 0; e < 16; e++) {
+            const uint32_t i = 16 * p + e;
+            t.w[i >> 2] |= gf16_mul_cx(e, inv) << (8 * (i & 3));
+        }
+    }
+    return t;
+}
+constexpr Gf16DivTable kGf16Div = gf16_div_table();
+__constant__ Gf16DivTable c_gf16_div = kGf16Div;
 __host__ __device__ __forceinline__ uint32_t gf16_inv_reg(uint32_t a) {
     return (uint32_t)(kGf16InvTable >> (4 * (a & 0xF))) & 0xFu;
 }

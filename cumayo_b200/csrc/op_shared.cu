@@ -683,7 +683,8 @@ static int verify_shared_t(const VerifyIO &io0, uint8_t *ws, size_t batch, cudaS
     uint8_t *tws = ws + WSL::inst_off();
     tl_tm.n = 0;
     tmark(st);
-    verify_hash_kernel<SET><<<(unsigned)((batch + 127) / 128), 128, 0, st>>>(io, tws, WSL::inst, (uint32_t)batch);
+    verify_hash_kernel<SET><<<(unsigned)((batch + HASH_NT - 1) / HASH_NT), HASH_NT, 0, st>>>(io, tws, WSL::inst,
+                                                                                       (uint32_t)batch);
     tmark(st);
     int rc = launch_product<SET, true>(io.epk, io.sig, io.sig_stride, ws, batch, st);
     if (rc != ST_OK) return rc;

@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(SignCfg<SET>::NT) sign_kernel(const SignIO io)
 template <int SET>
 static int sign_t(const SignIO &io, size_t batch, cudaStream_t st) {
     using C = SignCfg<SET>;
-    sign_hash_kernel<SET><<<(unsigned)((batch + 127) / 128), 128, 0, st>>>(io, (uint32_t)batch);
+    sign_hash_kernel<SET><<<(unsigned)((batch + HASH_NT - 1) / HASH_NT), HASH_NT, 0, st>>>(io, (uint32_t)batch);
     if (!set_smem_attr(sign_kernel<SET>, C::total)) return ST_CUDA;
     sign_kernel<SET><<<(unsigned)batch, C::NT, C::total, st>>>(io);
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
@@ -82,12 +82,12 @@ static int sign_t(const SignIO &io, size_t batch, cudaStream_t st) {
 
 int launch_sign_hash(int set, const SignIO &io, size_t batch, cudaStream_t st) {
     if (batch == 0) return ST_OK;
-    const unsigned g = (unsigned)((batch + 127) / 128);
+    const unsigned g = (unsigned)((batch + HASH_NT - 1) / HASH_NT);
     switch (set) {
-        case 1: sign_hash_kernel<1><<<g, 128, 0, st>>>(io, (uint32_t)batch); break;
-        case 2: sign_hash_kernel<2><<<g, 128, 0, st>>>(io, (uint32_t)batch); break;
-        case 3: sign_hash_kernel<3><<<g, 128, 0, st>>>(io, (uint32_t)batch); break;
-        case 5: sign_hash_kernel<5><<<g, 128, 0, st>>>(io, (uint32_t)batch); break;
+        case 1: sign_hash_kernel<1><<<g, HASH_NT, 0, st>>>(io, (uint32_t)batch); break;
+        case 2: sign_hash_kernel<2><<<g, HASH_NT, 0, st>>>(io, (uint32_t)batch); break;
+        case 3: sign_hash_kernel<3><<<g, HASH_NT, 0, st>>>(io, (uint32_t)batch); break;
+        case 5: sign_hash_kernel<5><<<g, HASH_NT, 0, st>>>(io, (uint32_t)batch); break;
         default: return ST_BAD_SET;
     }
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;

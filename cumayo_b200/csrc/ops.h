@@ -9,6 +9,10 @@
 
 namespace mayo {
 
+// Threads per CTA of the thread-per-instance hash kernels: their registers allow 8 such CTAs per
+// SM, so small CTAs spread a batch evenly over the 148 SMs (whole waves).
+constexpr int HASH_NT = 64;
+
 // Status codes shared with include/mayo_b200.h.
 enum : int {
     ST_OK = 0,

@@ -422,6 +422,10 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
         }
     }
     for (int i = tid; i < W * 4; i += NT) reinterpret_cast<uint32_t *>(rhsacc)[i] = 0;
+    // the division table for the elimination, in the V-mask area (free once M is formed)
+    uint8_t *s_div = reinterpret_cast<uint8_t *>(masks);
+    static_assert((size_t)S::v * J * 16 >= 256, "division table fits the mask area");
+    for (int i = tid; i < 64; i += NT) reinterpret_cast<uint32_t *>(s_div)[i] = c_gf16_div.w[i];
     __syncthreads();
 
     // ---- Gauss-Jordan in constant time.  Thread owns columns c = KO - (tid + NT q): the RHS on
@@ -468,8 +472,9 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
 #pragma unroll
         for (int w = 0; w < W; w++) my_oh[q][w] = 0;
     }
-    // The owner of a column computes its pivot (lowest unpivoted row with a nonzero entry), the
-    // inverse and F' = inv * (a + e_p), and publishes F' and the row one-hot in buffer pcx & 1.
+    // The owner of a column computes its pivot (lowest unpivoted row with a nonzero entry) a_p and
+    // publishes D = a + e_p, the row one-hot and a_p in buffer pcx & 1; a column with entry e in
+    // row p then takes col ^= (e / a_p) D, which is col ^= e F' with F' = a_p^-1 (a + e_p).
     auto publish = [&](int q, int pcx) {
         uint4 *buf = pivbuf + (pcx & 1) * (W + 2);
         uint32_t *ohw = reinterpret_cast<uint32_t *>(buf + W);  // oh[0..W), found at [7]
@@ -490,20 +495,18 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
             o2 |= col[q][w].p2 & oh[w];
             o3 |= col[q][w].p3 & oh[w];
         }
+        // a_p (0 when the column has no unpivoted nonzero entry: then oh = 0 and no column changes)
         const uint32_t piv = (uint32_t)(o0 != 0) | ((uint32_t)(o1 != 0) << 1) | ((uint32_t)(o2 != 0) << 2) |
                              ((uint32_t)(o3 != 0) << 3);
-        const uint4 inv_m = scalar_masks(gf16_inv_reg(piv) & found);
 #pragma unroll
         for (int w = 0; w < W; w++) {
             G4 ap = col[q][w];
             ap.p0 ^= oh[w];
-            G4 F = g4_zero();
-            g4_madd(F, ap, inv_m);
-            g4_st(buf + w, F);
+            g4_st(buf + w, ap);
             ohw[w] = oh[w];
             my_oh[q][w] = oh[w];
         }
-        ohw[7] = found;
+        ohw[7] = piv;
         my_has[q] = found;
     };
 #pragma unroll
@@ -524,14 +527,15 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
         // columns update, so each step needs one barrier and the owner's chain overlaps them.
         const uint4 *buf = pivbuf + (pc & 1) * (W + 2);
         const uint32_t *ohw = reinterpret_cast<const uint32_t *>(buf + W);
-        G4 F[W];
+        G4 D[W];
         uint32_t oh[W];
 #pragma unroll
         for (int w = 0; w < W; w++) {
-            F[w] = g4_ld(buf + w);
+            D[w] = g4_ld(buf + w);
             oh[w] = ohw[w];
             pivoted[w] |= oh[w];
         }
+        const uint8_t *drow = s_div + 16 * ohw[7];  // e / a_p
 #pragma unroll
         for (int q = 0; q < CPT; q++) {
             const int c = KO - (tid + NT * q);
@@ -544,10 +548,11 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
                 e2 |= col[q][w].p2 & oh[w];
                 e3 |= col[q][w].p3 & oh[w];
             }
-            const uint4 em = make_uint4(0u - (uint32_t)(e0 != 0), 0u - (uint32_t)(e1 != 0), 0u - (uint32_t)(e2 != 0),
-                                        0u - (uint32_t)(e3 != 0));
+            const uint32_t e = (uint32_t)(e0 != 0) | ((uint32_t)(e1 != 0) << 1) | ((uint32_t)(e2 != 0) << 2) |
+                               ((uint32_t)(e3 != 0) << 3);
+            const uint4 fm = scalar_masks(drow[e]);
 #pragma unroll
-            for (int w = 0; w < W; w++) g4_madd(col[q][w], F[w], em);
+            for (int w = 0; w < W; w++) g4_madd(col[q][w], D[w], fm);
             if (c == pc + 1 && c < KO) publish(q, c);
         }
         const int nw = (KO - 1 - pc) / 32 + 1;  // warps with a column > pc (or column pc + 1)

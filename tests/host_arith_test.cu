@@ -27,6 +27,11 @@ int main() {
         if (gf16_inv_reg(a) != gf16_inv_ct(a)) FAIL("gf16_inv_reg %u", a);
     }
     if (gf16_inv_ct(0) != 0) FAIL("inv(0)");
+    for (uint32_t p = 0; p < 16; p++)  // division table of the elimination: byte 16 p + e = e / p
+        for (uint32_t e = 0; e < 16; e++) {
+            const uint32_t i = 16 * p + e, d = (kGf16Div.w[i >> 2] >> (8 * (i & 3))) & 0xFF;
+            if (p == 0 ? d != 0 : ref_mul(d, p) != e) FAIL("gf16 div %u / %u", e, p);
+        }
     for (int it = 0; it < 2000; it++) {
         uint32_t w[4] = {rnd(), rnd(), rnd(), rnd()}, s = rnd() & 0xF;
         // packed -> planes: plane bit b holds coordinate 8*(b&3) + (b>>2)
