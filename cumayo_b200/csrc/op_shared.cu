@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
 // First attempt from the planes, in a CTA without engine staging (more CTAs per SM).  A singular
 // first attempt goes to the retry list; the fix-up kernel finishes it with the engine.
 template <int SET>
-__global__ void __launch_bounds__(SignCfg<SET>::NT)
+__global__ void __launch_bounds__(SignCfg<SET>::NT, SET == 5 ? 5 : 1)  // MAYO_5: 5 CTAs per SM by registers
     sign_shared_tail_kernel(const uint8_t *esk, uint8_t *sig, size_t sig_stride, const uint8_t *wsi, size_t wsi_stride,
                             const uint4 *planes, const uint4 *opl, uint32_t *ctl, uint32_t *retry) {
     using P = SharedProb<SET, false>;

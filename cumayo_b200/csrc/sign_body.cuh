@@ -141,10 +141,29 @@ __device__ __forceinline__ void sign_load_ws(uint8_t *smem, int tid, const uint8
     int *s_flag = reinterpret_cast<int *>(smem + C::off_flag);
     (void)masks; (void)bs; (void)acol; (void)xacc; (void)upk; (void)mpk; (void)pivbuf; (void)rhsacc; (void)ypk; (void)s_key; (void)s_t; (void)s_vr; (void)s_x; (void)s_flag;
     using WS = SignWs<SET>;
-    for (int i = tid; i < S::digest + S::sk; i += NT) s_key[i] = ws[WS::dig + i];
-    for (int i = tid; i < S::sk; i += NT) s_key[S::digest + S::sk + i] = esk[i];
-    for (int i = tid; i < NW * 4; i += NT) s_t[i] = i < S::menc ? ws[WS::t + i] : 0;
-    for (int i = tid; i < S::vr; i += NT) s_vr[i] = ws[WS::vr + i];
+    if (CP_) {
+        // compact tail: the workspace row is 16-byte aligned and padded to 16 bytes, so it comes
+        // in with one 16-byte load per thread (into the V-mask area, free until the attempt)
+        constexpr int NV = (WS::total + 15) / 16;
+        static_assert((size_t)NV <= (size_t)S::v * J, "workspace staging fits the mask area");
+#pragma unroll 1
+        for (int i = tid; i < NV; i += NT) masks[i] = reinterpret_cast<const uint4 *>(ws)[i];
+#pragma unroll 1
+        for (int i = tid; i < S::sk; i += NT) s_key[S::digest + S::sk + i] = esk[i];
+        __syncthreads();
+        const uint8_t *st = reinterpret_cast<const uint8_t *>(masks);
+#pragma unroll 1
+        for (int i = tid; i < S::digest + S::sk; i += NT) s_key[i] = st[WS::dig + i];
+#pragma unroll 1
+        for (int i = tid; i < NW * 4; i += NT) s_t[i] = i < S::menc ? st[WS::t + i] : 0;
+#pragma unroll 1
+        for (int i = tid; i < S::vr; i += NT) s_vr[i] = st[WS::vr + i];
+    } else {
+        for (int i = tid; i < S::digest + S::sk; i += NT) s_key[i] = ws[WS::dig + i];
+        for (int i = tid; i < S::sk; i += NT) s_key[S::digest + S::sk + i] = esk[i];
+        for (int i = tid; i < NW * 4; i += NT) s_t[i] = i < S::menc ? ws[WS::t + i] : 0;
+        for (int i = tid; i < S::vr; i += NT) s_vr[i] = ws[WS::vr + i];
+    }
     __syncthreads();
 }
 
@@ -375,8 +394,33 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
             for (int j = 0; j < S::k; j++) {
                 const int ell = i <= j ? ell_of(i, j, S::k) : ell_of(j, i, S::k);
                 const uint32_t *u = mpk + ((size_t)j * S::o + b) * NW;
+                if constexpr (NW <= 10) {
+                    // z^ell u without the fold: the packed words shifted up by 4 ell bits -- a
+                    // funnel shift by the sub-word part, then a barrel shift by whole words (ell
+                    // is below k(k+1)/2, so at most QMAX words) -- coordinates >= m dropped.
+                    // (Larger sets keep the per-word form: fewer live registers.)
+                    constexpr int QMAX = (S::k * (S::k + 1) / 2 - 1) >> 3;
+                    const uint32_t sh = (uint32_t)(ell & 7) * 4u;
+                    const int Q = ell >> 3;
+                    uint32_t v[NW];
 #pragma unroll
-                for (int q = 0; q < NW; q++) acc[q] ^= zshift_word<SET>(u, q, ell);
+                    for (int q = 0; q < NW; q++) v[q] = u[q];
+#pragma unroll
+                    for (int q = NW - 1; q >= 0; q--) v[q] = __funnelshift_l(q > 0 ? v[q - 1] : 0u, v[q], sh);
+#pragma unroll
+                    for (int st = 1; st <= QMAX; st <<= 1) {
+                        const bool take = (Q & st) != 0;
+#pragma unroll
+                        for (int q = NW - 1; q >= 0; q--) v[q] = take ? (q >= st ? v[q - st] : 0u) : v[q];
+                    }
+                    if (S::m % 8) v[S::m / 8] &= (1u << (4 * (S::m % 8))) - 1u;
+#pragma unroll
+                    for (int q = 0; q < NW; q++)
+                        if (q < (S::m + 7) / 8) acc[q] ^= v[q];
+                } else {
+#pragma unroll
+                    for (int q = 0; q < NW; q++) acc[q] ^= zshift_word<SET>(u, q, ell);
+                }
                 if (ell > 0) {
                     // overflow coordinates m-ell..m-1 -> 0..ell-1, times z^n * c_n for n = 0..3;
                     // ell < k(k+1)/2, so only the first OVW packed words can hold overflow and
