@@ -15,14 +15,15 @@
 // Kernels:
 //   shared_a_kernel     builds A from the key, tiled for the MMA (one 128-row tile = the four bit
 //                       planes of one 32-coordinate group of one row r) in the K-major, no-swizzle
-//                       shared-memory layout, so a tile moves to shared memory with one bulk copy.
-//   shared_gemm_kernel  one CTA per N instances' vectors (B, built in shared memory from their
-//                       nibbles, resident): for every A tile, a bulk copy (double-buffered), one
-//                       thread issues the MMAs into a TMEM accumulator (double-buffered), and eight
-//                       warps read the accumulator back (tcgen05.ld, 16-bit halves), gather bit 7
-//                       of 32 sums into one word -- one 32-coordinate bit plane -- and store the
-//                       planes.  Zero blocks of A (columns c < r of the triangular P1 / P) are
-//                       skipped.  Waits are bounded: a timeout sets the status word and unwinds.
+//                       shared-memory layout, so a run of k-steps of a tile moves to shared memory
+//                       with one bulk copy; for sign also the key's O planes.
+//   shared_gemm_kernel  one CTA per 256 instance vectors (B, built in shared memory from their
+//                       nibbles, resident): a loader warp streams A through a ring of chunks, two
+//                       issuer warps run the MMAs of alternate tiles into two TMEM accumulators,
+//                       and eight warps read an accumulator back (tcgen05.ld, 16-bit halves),
+//                       gather bit 7 of 32 sums into one word -- one 32-coordinate bit plane -- and
+//                       store the planes.  Zero blocks of A (columns c < r of the triangular P1 / P)
+//                       are skipped.  Waits are bounded: a timeout sets the status word and unwinds.
 //   sign: sign_hash_kernel (thread per instance) -> product -> sign_shared_tail_kernel (first
 //         attempt from the planes in a compact CTA) -> sign_shared_fix_kernel (retries of the
 //         rare singular first attempts with the engine).
