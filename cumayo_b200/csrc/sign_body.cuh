@@ -4,9 +4,11 @@
 //   U = V^T P1 V and y = sum z^l U_l + t        engine over P1 rows          (sign.cu:396-460)
 //   M_i = V_i L                                  engine over the columns of L (sign.cu:256-330)
 //   A = sum z^l M                                packed z-shifts, one thread per column (sign.cu:333-393)
-//   x = solve(A, y, r)                           constant-time Gauss-Jordan over bit-planes (sign.cu:10-145)
-// Every value derived from the secret key enters arithmetic only through masks, so no branch
-// or shared-memory address depends on it; only the attempt count is data dependent, as in MAYO.
+//   x = solve(A, y, r)                           Gauss-Jordan over bit-planes, no data branches (sign.cu:10-145)
+// No branch depends on a value derived from the secret key; only the attempt count is data
+// dependent, as in MAYO.  One shared-memory read depends on the data: the elimination's
+// 256-byte division table at index (a_p, e); the reference's elimination (sign.cu:48-100)
+// branches on the entries and reads its multiplication table the same way.
 //
 // Why the elimination may differ from the reference's and still give identical bytes: when
 // rank A = m, the reference's pivot columns are the lexicographically first column basis of A
@@ -472,7 +474,7 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
     for (int i = tid; i < 64; i += NT) reinterpret_cast<uint32_t *>(s_div)[i] = c_gf16_div.w[i];
     __syncthreads();
 
-    // ---- Gauss-Jordan in constant time.  Thread owns columns c = KO - (tid + NT q): the RHS on
+    // ---- Gauss-Jordan without data branches.  Thread owns columns c = KO - (tid + NT q): the RHS on
     // thread 0 and the columns still to update (c > pc) on the lowest threads, so the work of a
     // step stays in as few warps as possible. ----
     G4 col[CPT][W];
