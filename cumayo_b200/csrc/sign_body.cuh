@@ -392,6 +392,16 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
         for (int q = 0; q < NW; q++) acc[q] = 0;
         if (c < KO) {
             const int i = c / S::o, b = c - i * S::o;
+            // The overflow of each z^ell M_j (coordinates m-ell..m-1, moved to 0..ell-1) is
+            // summed over j and folded by f(z) once: the fold is linear.  ell < k(k+1)/2, so only
+            // the first OVW packed words can hold overflow, and the fold (shifts by n < 4
+            // coordinates) touches only the first FW words.
+            constexpr int ELL_MAX = S::k * (S::k + 1) / 2 - 1;
+            constexpr int OVW = (ELL_MAX + 7) / 8 < NW ? (ELL_MAX + 7) / 8 : NW;
+            constexpr int FW = OVW + 1 < NW ? OVW + 1 : NW;
+            uint32_t ovs[OVW];
+#pragma unroll
+            for (int q = 0; q < OVW; q++) ovs[q] = 0;
 #pragma unroll 1
             for (int j = 0; j < S::k; j++) {
                 const int ell = i <= j ? ell_of(i, j, S::k) : ell_of(j, i, S::k);
@@ -424,33 +434,27 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
                     for (int q = 0; q < NW; q++) acc[q] ^= zshift_word<SET>(u, q, ell);
                 }
                 if (ell > 0) {
-                    // overflow coordinates m-ell..m-1 -> 0..ell-1, times z^n * c_n for n = 0..3;
-                    // ell < k(k+1)/2, so only the first OVW packed words can hold overflow and
-                    // the fold (shifts by n < 4 coordinates) touches only the first FW words
-                    constexpr int ELL_MAX = S::k * (S::k + 1) / 2 - 1;
-                    constexpr int OVW = (ELL_MAX + 7) / 8 < NW ? (ELL_MAX + 7) / 8 : NW;
-                    constexpr int FW = OVW + 1 < NW ? OVW + 1 : NW;
-                    uint32_t ov[OVW];
-#pragma unroll
-                    for (int q = 0; q < OVW; q++) ov[q] = zdown_word<SET>(u, q, S::m - ell);
-                    // mask coordinates >= ell
+                    // overflow coordinates m-ell..m-1 -> 0..ell-1 (coordinates >= ell masked)
 #pragma unroll
                     for (int q = 0; q < OVW; q++) {
+                        uint32_t ov = zdown_word<SET>(u, q, S::m - ell);
                         const int lo = 8 * q;
-                        if (lo >= ell) ov[q] = 0;
-                        else if (lo + 8 > ell) ov[q] &= (1u << (4 * (ell - lo))) - 1;
+                        if (lo >= ell) ov = 0;
+                        else if (lo + 8 > ell) ov &= (1u << (4 * (ell - lo))) - 1;
+                        ovs[q] ^= ov;
                     }
+                }
+            }
+            // + sum_n c_n z^n (overflow): the reduction by f(z) = z^m + sum_n c_n z^n
 #pragma unroll
-                    for (int n = 0; n < 4; n++) {
-                        if (S::cf(n) == 0) continue;
-                        uint32_t prev = 0;
+            for (int n = 0; n < 4; n++) {
+                if (S::cf(n) == 0) continue;
+                uint32_t prev = 0;
 #pragma unroll
-                        for (int q = 0; q < FW; q++) {
-                            const uint32_t mc = q < OVW ? nib8_mul_const(ov[q], S::cf(n)) : 0u;
-                            acc[q] ^= n ? ((mc << (4 * n)) | (prev >> (32 - 4 * n))) : mc;
-                            prev = mc;
-                        }
-                    }
+                for (int q = 0; q < FW; q++) {
+                    const uint32_t mc = q < OVW ? nib8_mul_const(ovs[q], S::cf(n)) : 0u;
+                    acc[q] ^= n ? ((mc << (4 * n)) | (prev >> (32 - 4 * n))) : mc;
+                    prev = mc;
                 }
             }
         } else {
