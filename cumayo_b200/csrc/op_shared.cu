@@ -75,7 +75,11 @@ struct SharedProb {
     static constexpr size_t SLOT = (size_t)2 * KROWS * 16;  // one k-step of key rows: [2][KROWS][16 B]
     static constexpr size_t BAR_BYTES = 1024;               // mbarriers (2 NCH + 6) and flags
     static constexpr int nch_fit(int ck) { return (int)((SH_SMEM_MAX - (size_t)NINST * KPAD - BAR_BYTES) / (ck * SLOT)); }
-    static constexpr int CK = nch_fit(8) >= 3 ? 8 : 4;      // k-steps per chunk
+    // k-steps per chunk: a tile's k-steps in near-equal chunks of at most 8 (MAYO_2 verify, 11
+    // k-steps: 6 + 5 takes 0.96 ms where 8 + 3 takes 0.99), or 4 when fewer than three 8-step
+    // chunks fit beside the vectors
+    static constexpr int CK_EVEN = (KSTEPS + (KSTEPS + 7) / 8 - 1) / ((KSTEPS + 7) / 8);
+    static constexpr int CK = nch_fit(8) >= 3 ? CK_EVEN : 4;
     static constexpr int NCH_FIT = nch_fit(CK);
     static constexpr int NCH = NCH_FIT < 16 ? NCH_FIT : 16;
     static_assert(NCH >= 2, "key ring");
