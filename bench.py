@@ -69,8 +69,8 @@ KERNEL_ROOF_DEF = {
 # instances) from one ncu capture of the MAYO_2 shared-key kernels at 16,384 instances
 # (profiles/sign_tail_mayo2_shared_b16384.md, profiles/product_gemm_mayo2_shared_b16384.md);
 # the traffic grows in proportion to the instances, so a launch's traffic is this x its batch.
-KERNEL_TRAFFIC_PER_INST = {2: {"sign.tail": 180.400896e6 / 16384, "verify.tail": 177.768704e6 / 16384,
-                               "sign.product": 132.78592e6 / 16384, "verify.product": 130.78272e6 / 16384}}
+KERNEL_TRAFFIC_PER_INST = {2: {"sign.tail": 179.689728e6 / 16384, "verify.tail": 177.242624e6 / 16384,
+                               "sign.product": 130.477568e6 / 16384, "verify.product": 128.245248e6 / 16384}}
 
 # ---------------------------------------------------------------------------------------------
 # workloads
