@@ -71,6 +71,9 @@ KERNEL_ROOF_DEF = {
 # the traffic grows in proportion to the instances, so a launch's traffic is this x its batch.
 KERNEL_TRAFFIC_PER_INST = {2: {"sign.tail": 179.689728e6 / 16384, "verify.tail": 177.242624e6 / 16384,
                                "sign.product": 130.477568e6 / 16384, "verify.product": 128.245248e6 / 16384}}
+# The same for verify_kernel<SET> on distinct keys (one capture of 4,096 instances per set,
+# profiles/verify_distinct_mayo3_mayo5_b4096.md): the instance's EPK is read once.
+VERIFY_TRAFFIC_PER_INST = {3: (1.557413e9 + 4.978176e6) / 4096, 5: (3.478466e9 + 4.699392e6) / 4096}
 
 # ---------------------------------------------------------------------------------------------
 # workloads
@@ -603,7 +606,9 @@ def run_ours(args, dist: Dist):
         "roofline_hbm": {"bound": "hbm", "kernel": f"{dom} ({args.workload})",
                          "achieved": round(hbm_bytes[dom] / (phase_ms[dom] / 1e3) / 1e9, 2),
                          "peak": HBM_PEAK_GBS, "unit": "GB/s",
-                         "frac": round(hbm_bytes[dom] / (phase_ms[dom] / 1e3) / 1e9 / HBM_PEAK_GBS, 5), "traffic": None,
+                         "frac": round(hbm_bytes[dom] / (phase_ms[dom] / 1e3) / 1e9 / HBM_PEAK_GBS, 5),
+                         "traffic": (int(VERIFY_TRAFFIC_PER_INST[s] * batch)
+                                     if wl["kind"] == "distinct_verify" and s in VERIFY_TRAFFIC_PER_INST else None),
                          "definition": "algorithmic bytes the kernel must move from HBM per launch / kernel time; "
                                        f"peak = copy bandwidth ({HBM_PEAK_SRC})"},
         "e2e": {"value": round(ops_per_step * dist.world / (e2e_ms / args.steps / 1e3), 1), "unit": "ops/s",
