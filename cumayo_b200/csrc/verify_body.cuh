@@ -25,8 +25,10 @@ struct VerifyCfg {
     static_assert(R >= 1 && J * W * R <= NC, "engine threads");
     static constexpr size_t off_masks = 0;
     static constexpr size_t off_bs = off_masks + (size_t)S::n * J * 16;
-    static constexpr size_t off_x = off_bs + (size_t)R * S::n * W * 16;
-    static constexpr size_t off_upk = off_x + (size_t)J * J * W * 16;
+    // the U accumulators reuse the key-row staging area once the row loop is done
+    static constexpr size_t off_x = off_bs;
+    static constexpr size_t sz_bs = (size_t)R * S::n * W * 16, sz_x = (size_t)J * J * W * 16;
+    static constexpr size_t off_upk = off_bs + (sz_bs > sz_x ? sz_bs : sz_x);
     static constexpr size_t off_sig = off_upk + pad16((size_t)S::pairs * NW * 4);
     static constexpr size_t off_key = off_sig + pad16(S::sig);
     static constexpr size_t off_t = off_key + pad16(S::digest + S::sk);
@@ -72,7 +74,6 @@ __device__ __forceinline__ void verify_instance(uint8_t *smem, int tid, const ui
     uint8_t *s_t = smem + C::off_t;
 
     for (int i = tid; i < S::sig; i += C::NT) s_sig[i] = sig[i];
-    for (int i = tid; i < J * J * W * 4; i += C::NT) reinterpret_cast<uint32_t *>(xacc)[i] = 0;
     for (int i = tid; i < NW * 4; i += C::NT) s_t[i] = 0;
     __syncthreads();
 
@@ -126,6 +127,10 @@ __device__ __forceinline__ void verify_instance(uint8_t *smem, int tid, const ui
                 bar_sync(1, NC);
             }
         }
+        // the staging area is free now (the last row pass ended with a barrier): zero the
+        // accumulators there, then combine the threads' partial sums
+        for (int i = tid; i < J * J * W * 4; i += NC) reinterpret_cast<uint32_t *>(xacc)[i] = 0;
+        bar_sync(1, NC);
         if (eng.active) {
 #pragma unroll
             for (int i = 0; i < J; i++) g4_atomic_xor(xacc + ((size_t)i * J + eng.j) * W + eng.w, X[i]);
