@@ -25,11 +25,14 @@ struct VerifyCfg {
     static_assert(R >= 1 && J * W * R <= NC, "engine threads");
     static constexpr size_t off_masks = 0;
     static constexpr size_t off_bs = off_masks + (size_t)S::n * J * 16;
-    // the U accumulators reuse the key-row staging area once the row loop is done
+    // the U accumulators, then U's packed words, reuse the key-row staging area once the row
+    // loop is done (in place after it when they do not fit)
     static constexpr size_t off_x = off_bs;
     static constexpr size_t sz_bs = (size_t)R * S::n * W * 16, sz_x = (size_t)J * J * W * 16;
-    static constexpr size_t off_upk = off_bs + (sz_bs > sz_x ? sz_bs : sz_x);
-    static constexpr size_t off_sig = off_upk + pad16((size_t)S::pairs * NW * 4);
+    static constexpr size_t sz_upk = pad16((size_t)S::pairs * NW * 4);
+    static constexpr bool UPK_IN_BS = sz_x + sz_upk <= sz_bs;
+    static constexpr size_t off_upk = UPK_IN_BS ? off_bs + sz_x : off_bs + (sz_bs > sz_x ? sz_bs : sz_x);
+    static constexpr size_t off_sig = UPK_IN_BS ? off_bs + sz_bs : off_upk + sz_upk;
     static constexpr size_t off_key = off_sig + pad16(S::sig);
     static constexpr size_t off_t = off_key + pad16(S::digest + S::sk);
     static constexpr size_t total = off_t + pad16(NW * 4);
