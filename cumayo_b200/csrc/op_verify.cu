@@ -6,12 +6,21 @@
 namespace mayo {
 
 template <int SET>
-__global__ void __launch_bounds__(VerifyCfg<SET>::NT) verify_kernel(const VerifyIO io) {
+__device__ __forceinline__ void verify_cta(const VerifyIO &io) {
     extern __shared__ __align__(16) uint8_t smem[];
     const size_t inst = blockIdx.x;
     verify_instance<SET, VerifyCfg<SET>::NC>(smem, threadIdx.x, io.epk + inst * io.epk_stride, io.m.ptr(inst),
                                              io.m.len(inst), io.sig + inst * io.sig_stride,
                                              io.res + inst * io.res_stride);
+}
+template <int SET>
+__global__ void __launch_bounds__(VerifyCfg<SET>::NT) verify_kernel(const VerifyIO io) {
+    verify_cta<SET>(io);
+}
+// MAYO_3: its shared memory allows 6 CTAs per SM; registers capped to match
+template <>
+__global__ void __launch_bounds__(VerifyCfg<3>::NT, 6) verify_kernel<3>(const VerifyIO io) {
+    verify_cta<3>(io);
 }
 
 template <int SET>
