@@ -49,8 +49,12 @@ struct SignCfg {
     static constexpr size_t off_bs = off_masks + (size_t)S::v * J * 16;
     static constexpr size_t sz_bs = COMPACT ? 0 : (size_t)R * S::n * W * 16;
     static constexpr size_t sz_acol = (size_t)NCOL * W * 16;
-    static constexpr size_t off_x = off_bs + (sz_bs > sz_acol ? sz_bs : sz_acol);
-    static constexpr size_t off_upk = off_x + (size_t)J * J * W * 16;
+    static constexpr size_t sz_x = (size_t)J * J * W * 16;
+    // With engine staging, the U accumulators reuse it: they are written after the U loop's last
+    // read of the staging area and consumed before the M loop's first write.
+    static constexpr bool X_IN_BS = !COMPACT && sz_bs >= sz_x;
+    static constexpr size_t off_x = X_IN_BS ? off_bs : off_bs + (sz_bs > sz_acol ? sz_bs : sz_acol);
+    static constexpr size_t off_upk = X_IN_BS ? off_bs + (sz_bs > sz_acol ? sz_bs : sz_acol) : off_x + sz_x;
     static constexpr size_t off_mpk = off_upk + pad16((size_t)S::pairs * NW * 4);
     static constexpr size_t off_piv = off_mpk + pad16((size_t)S::k * S::o * NW * 4);
     static constexpr size_t off_rhs = off_piv + (size_t)2 * (W + 2) * 16;
@@ -278,17 +282,15 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
         const int q = i * S::m + c;
         masks[idx] = scalar_masks((s_vr[q >> 1] >> ((q & 1) * 4)) & 0xF);
     }
-    for (int i = tid; i < J * J * W * 4; i += NT) reinterpret_cast<uint32_t *>(xacc)[i] = 0;
     __syncthreads();
 
-    // ---- U = V^T P1 V ----
+    // ---- U = V^T P1 V: X[i][j] = sum_r V_i[r] T_j[r]; thread (j, w, rs) takes rows rs, rs + R, ... ----
+    G4 X[J];
+#pragma unroll
+    for (int i = 0; i < J; i++) X[i] = g4_zero();
     if (CP_ || pre) {  // a compact CTA has no engine staging: precomputed products only
-        // X[i][j] = sum_r V_i[r] T_j[r]: thread (j, w, rs) takes rows rs, rs + R, ...
         constexpr int NROWS = S::v + S::o;
         if (eng.active) {
-            G4 X[J];
-#pragma unroll
-            for (int i = 0; i < J; i++) X[i] = g4_zero();
 #pragma unroll 1
             for (int r = eng.rs; r < S::v; r += R) {
                 const G4 T = g4_ld(pre + ((size_t)eng.j * NROWS + r) * W + eng.w);
@@ -296,14 +298,9 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
 #pragma unroll
                 for (int i = 0; i < J; i++) g4_madd(X[i], T, mr[i]);
             }
-#pragma unroll
-            for (int i = 0; i < J; i++) g4_atomic_xor(xacc + ((size_t)i * J + eng.j) * W + eng.w, X[i]);
         }
     } else {
         const P1Rows<SET> rows{P1};
-        G4 X[J];
-#pragma unroll
-        for (int i = 0; i < J; i++) X[i] = g4_zero();
 #pragma unroll 1
         for (int r0 = 0; r0 < S::v; r0 += R) {
             eng.convert(rows, r0, S::v, tid, NT);
@@ -317,10 +314,14 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
             }
             __syncthreads();
         }
-        if (eng.active) {
+    }
+    // the accumulators may share the engine staging area, whose last read is behind the loop's
+    // final barrier: zero them, then combine the threads' partial sums
+    for (int i = tid; i < J * J * W * 4; i += NT) reinterpret_cast<uint32_t *>(xacc)[i] = 0;
+    __syncthreads();
+    if (eng.active) {
 #pragma unroll
-            for (int i = 0; i < J; i++) g4_atomic_xor(xacc + ((size_t)i * J + eng.j) * W + eng.w, X[i]);
-        }
+        for (int i = 0; i < J; i++) g4_atomic_xor(xacc + ((size_t)i * J + eng.j) * W + eng.w, X[i]);
     }
     __syncthreads();
     for (int idx = tid; idx < S::pairs * W; idx += NT) {
