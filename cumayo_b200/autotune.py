@@ -45,6 +45,19 @@ def signature(items: np.ndarray) -> str:
     return "q:" + ",".join(str(int(c)) for c in counts)
 
 
+def cache_key(gpu_name: str, sms: int, per_max: dict, items: np.ndarray) -> str:
+    """Cache key: the GPU, the SMs used, every bucket's resident CTAs per SM (the kernels' register
+    and shared-memory budgets: a library built with other budgets must not replay shapes tuned
+    for another one) and the workload signature."""
+    occ = ",".join(f"{s}/{op}={per_max[(s, op)]}" for (s, op) in sorted(per_max))
+    return f"{gpu_name}|sms={sms}|occ={occ}|{signature(items)}"
+
+
+def clamp_shape(ctas_per_sm: dict, per_max: dict) -> dict:
+    """A shape's CTAs per SM, each within 1 .. the bucket's residency."""
+    return {b: max(1, min(int(c), int(per_max.get(b, c)))) for b, c in ctas_per_sm.items()}
+
+
 def _time(q: "Q.Queue", repeats: int) -> float:
     import torch
     q.run()
@@ -67,7 +80,7 @@ def tune_queue(q: "Q.Queue", items: np.ndarray, repeats: int = 2, use_cache: boo
     dev = torch.cuda.current_device()
     name = torch.cuda.get_device_name(dev)
     per_max = {b: Q.ctas_per_sm(*b) for b in Q.BUCKETS}
-    key = f"{name}|sms={q.shape.sms}|{signature(items)}"
+    key = cache_key(name, q.shape.sms, per_max, items)
     cache = _load() if use_cache else {}
     q.load(items)
     if key in cache:
@@ -90,7 +103,7 @@ def tune_queue(q: "Q.Queue", items: np.ndarray, repeats: int = 2, use_cache: boo
         cache[key] = best
         if use_cache:
             _store(cache)
-    q.shape = Q.Shape(sms=q.shape.sms,
-                      ctas_per_sm={tuple(int(x) for x in k.split("/")): c for k, c in best["ctas_per_sm"].items()},
+    cps = {tuple(int(x) for x in k.split("/")): c for k, c in best["ctas_per_sm"].items()}
+    q.shape = Q.Shape(sms=q.shape.sms, ctas_per_sm=clamp_shape(cps, per_max),
                       launch_order=[tuple(b) for b in best["order_buckets"]])
     return best
