@@ -209,6 +209,58 @@ struct Sponge {
     // Absorb `len` bytes from any generic address (global, shared or local).  The state stays
     // in registers: every state word is addressed with a compile-time index.
     __device__ void absorb(const uint8_t *p, uint32_t len) {
+        // Global memory from the start of a block: aligned 8-byte loads, each word of the block
+        // funnel-shifted out of two of them (one new load per word), instead of one load per byte
+        // of an unaligned message.  Every aligned word read holds at least one input byte, so no
+        // read leaves the pages the input lies in; bytes outside the input are masked off.
+        const bool aligned_path = __isGlobal(p) != 0;
+        while (aligned_path && pos == 0 && len >= (uint32_t)RATE) {
+            const uint32_t off = (uint32_t)(reinterpret_cast<uintptr_t>(p) & 7u);
+            const uint64_t *q = reinterpret_cast<const uint64_t *>(p - off);
+            if (off == 0) {
+#pragma unroll
+                for (int i = 0; i < RW; i++) s[i] ^= q[i];
+            } else {
+                const uint32_t sh = 8u * off;
+                uint64_t w0 = q[0];
+#pragma unroll
+                for (int i = 0; i < RW; i++) {
+                    const uint64_t w1 = q[i + 1];
+                    s[i] ^= (w0 >> sh) | (w1 << (64u - sh));
+                    w0 = w1;
+                }
+            }
+            keccak_f1600(s);
+            p += RATE;
+            len -= RATE;
+        }
+        if (aligned_path && pos == 0 && len > 0) {  // a last partial block (len < RATE)
+            const uint32_t off = (uint32_t)(reinterpret_cast<uintptr_t>(p) & 7u);
+            const uint64_t *q = reinterpret_cast<const uint64_t *>(p - off);
+            const int n = (int)len;
+            const uint32_t sh = 8u * off;
+            uint64_t w0 = q[0];
+#pragma unroll
+            for (int i = 0; i < RW; i++) {
+                if (8 * i < n) {
+                    uint64_t v;
+                    if (off == 0) {
+                        v = i ? q[i] : w0;
+                    } else {
+                        // the word's last input byte lies in the next aligned word, or the input
+                        // ends inside this one (and no later word has input bytes)
+                        const int last = min(8 * i + 7, n - 1);
+                        const uint64_t w1 = (int)off + last >= 8 * (i + 1) ? q[i + 1] : 0ull;
+                        v = (w0 >> sh) | (w1 << (64u - sh));
+                        w0 = w1;
+                    }
+                    if (8 * i + 8 > n) v &= ~0ull >> (64 - 8 * (n - 8 * i));
+                    s[i] ^= v;
+                }
+            }
+            pos = n;
+            return;
+        }
         while (len > 0) {
             const int take = min((int)len, RATE - pos);
 #pragma unroll
