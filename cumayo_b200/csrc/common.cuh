@@ -261,6 +261,24 @@ struct Sponge {
             pos = n;
             return;
         }
+        if ((reinterpret_cast<uintptr_t>(p) & 7) == 0 && ((pos | (int)len) & 7) == 0) {
+            // whole aligned words at a word position (any memory space: exactly the input's words)
+            const uint64_t *q = reinterpret_cast<const uint64_t *>(p);
+            while (len > 0) {
+                const int take = min((int)len, RATE - pos);
+#pragma unroll
+                for (int i = 0; i < RW; i++)
+                    if (8 * i >= pos && 8 * i < pos + take) s[i] ^= q[i - (pos >> 3)];
+                q += take >> 3;
+                pos += take;
+                len -= take;
+                if (pos == RATE) {
+                    keccak_f1600(s);
+                    pos = 0;
+                }
+            }
+            return;
+        }
         while (len > 0) {
             const int take = min((int)len, RATE - pos);
 #pragma unroll
@@ -302,13 +320,28 @@ struct Sponge {
             }
             const int take = min((int)len, RATE - pos);
             const int lo = pos, hi = pos + take;
+            if ((pos & 7) == 0 && (reinterpret_cast<uintptr_t>(out) & 7) == 0) {
+                // aligned output: whole state words as 8-byte stores, then the last bytes
+                uint64_t *o64 = reinterpret_cast<uint64_t *>(out);
 #pragma unroll
-            for (int i = 0; i < RW; i++)
+                for (int i = 0; i < RW; i++) {
+                    if (8 * i >= lo && 8 * i + 8 <= hi) {
+                        o64[i - (lo >> 3)] = s[i];
+                    } else if (8 * i >= lo && 8 * i < hi) {
 #pragma unroll
-                for (int b = 0; b < 8; b++) {
-                    const int bp = 8 * i + b;
-                    if (bp >= lo && bp < hi) out[bp - lo] = (uint8_t)(s[i] >> (8 * b));
+                        for (int b = 0; b < 8; b++)
+                            if (8 * i + b < hi) out[8 * i + b - lo] = (uint8_t)(s[i] >> (8 * b));
+                    }
                 }
+            } else {
+#pragma unroll
+                for (int i = 0; i < RW; i++)
+#pragma unroll
+                    for (int b = 0; b < 8; b++) {
+                        const int bp = 8 * i + b;
+                        if (bp >= lo && bp < hi) out[bp - lo] = (uint8_t)(s[i] >> (8 * b));
+                    }
+            }
             out += take;
             len -= take;
             pos += take;

@@ -494,7 +494,7 @@ __global__ void verify_hash_kernel(const VerifyIO io, uint8_t *tws, size_t tws_s
     using S = Set<SET>;
     const uint32_t inst = blockIdx.x * blockDim.x + threadIdx.x;
     if (inst >= batch) return;
-    uint8_t digest[S::digest];
+    alignas(8) uint8_t digest[S::digest];
     Sponge<136> sp;
     sp.init();
     sp.absorb(io.m.ptr(inst), io.m.len(inst));

@@ -16,7 +16,8 @@ __global__ void sign_hash_kernel(const SignIO io, uint32_t batch) {
     if (inst >= batch) return;
     const uint8_t *seed_sk = io.esk + (size_t)inst * io.esk_stride;
     uint8_t *ws = io.ws + (size_t)inst * io.ws_stride;
-    uint8_t digest[S::digest], salt[S::sk];
+    alignas(8) uint8_t digest[S::digest];
+    alignas(8) uint8_t salt[S::sk];
     {
         Sponge<136> sp;  // digest = SHAKE256(M) (sign.cu:225)
         sp.init();
@@ -51,8 +52,16 @@ __global__ void sign_hash_kernel(const SignIO io, uint32_t batch) {
         sp.finalize();
         sp.squeeze(ws + WS::vr, S::vr);
     }
-    for (int i = 0; i < S::digest; i++) ws[WS::dig + i] = digest[i];
-    for (int i = 0; i < S::sk; i++) ws[WS::salt + i] = salt[i];
+    static_assert(WS::dig % 8 == 0 && WS::salt % 8 == 0 && S::digest % 8 == 0 && S::sk % 8 == 0, "word copies");
+    if ((reinterpret_cast<uintptr_t>(ws) & 7) == 0) {  // the shared-key workspace; pool scratch may be unaligned
+        for (int i = 0; i < S::digest / 8; i++)
+            reinterpret_cast<uint64_t *>(ws + WS::dig)[i] = reinterpret_cast<const uint64_t *>(digest)[i];
+        for (int i = 0; i < S::sk / 8; i++)
+            reinterpret_cast<uint64_t *>(ws + WS::salt)[i] = reinterpret_cast<const uint64_t *>(salt)[i];
+    } else {
+        for (int i = 0; i < S::digest; i++) ws[WS::dig + i] = digest[i];
+        for (int i = 0; i < S::sk; i++) ws[WS::salt + i] = salt[i];
+    }
 }
 
 template <int SET>
