@@ -303,14 +303,15 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
             const uint32_t inst = inst0 + (uint32_t)(n / S::k);
             const int j = n % S::k;
             uint32_t wd[4] = {0u, 0u, 0u, 0u};
-            if (n < P::NI * S::k && inst < batch) {
-                const uint8_t *vp = vec + (size_t)inst * vec_stride;
+            if (n < P::NI * S::k && inst < batch && 4 * ch < P::NVEC) {
+                // the chunk's four nibbles from one little-endian word (aligned loads; the bytes
+                // after a vector are the next vector's, r's or the salt's, so all four exist)
+                const int nib0 = j * P::NVEC + 4 * ch;
+                const uint32_t x4 = ld_le32(vec + (size_t)inst * vec_stride + (nib0 >> 1)) >> ((nib0 & 1) * 4);
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
-                    const int c = 4 * ch + q;
-                    if (c < P::NVEC) {
-                        const int nib = j * P::NVEC + c;
-                        const uint32_t x = (vp[nib >> 1] >> ((nib & 1) * 4)) & 0xFu;
+                    if (4 * ch + q < P::NVEC) {
+                        const uint32_t x = (x4 >> (4 * q)) & 0xFu;
                         wd[q] = (x * 0x00204081u) & 0x01010101u;  // bit b' -> byte b'
                     }
                 }
