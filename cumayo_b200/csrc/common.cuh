@@ -295,6 +295,18 @@ struct Sponge {
             }
         }
     }
+    // Absorb n zero bytes: XOR with zero leaves the state; only the position moves.
+    __device__ __forceinline__ void absorb_zeros(int n) {
+        while (n > 0) {
+            const int take = min(n, RATE - pos);
+            pos += take;
+            n -= take;
+            if (pos == RATE) {
+                keccak_f1600(s);
+                pos = 0;
+            }
+        }
+    }
     __device__ __forceinline__ void absorb_byte(uint8_t b) {
 #pragma unroll
         for (int i = 0; i < RW; i++)

@@ -29,7 +29,7 @@ __global__ void sign_hash_kernel(const SignIO io, uint32_t batch) {
         Sponge<136> sp;  // salt = SHAKE256(digest || 0^SK || seed_sk) (sign.cu:230-238)
         sp.init();
         sp.absorb(digest, S::digest);
-        for (int i = 0; i < S::sk; i++) sp.absorb_byte(0);
+        sp.absorb_zeros(S::sk);
         sp.absorb(seed_sk, S::sk);
         sp.finalize();
         sp.squeeze(salt, S::sk);
@@ -48,7 +48,7 @@ __global__ void sign_hash_kernel(const SignIO io, uint32_t batch) {
         sp.absorb(digest, S::digest);
         sp.absorb(salt, S::sk);
         sp.absorb(seed_sk, S::sk);
-        sp.absorb_byte(0);
+        sp.absorb_zeros(1);  // ctr = 0
         sp.finalize();
         sp.squeeze(ws + WS::vr, S::vr);
     }
