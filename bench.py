@@ -128,35 +128,49 @@ def seeds_for(seed: int, batch: int, skb: int) -> np.ndarray:
 # distributed plumbing (one process per GPU)
 # ---------------------------------------------------------------------------------------------
 class Dist:
+    """One process per GPU (torchrun's env); NCCL, or `gloo` (MAYO_BENCH_DIST_BACKEND) for the
+    CPU tests of the multi-rank plumbing.  No collective touches the data path: ranks meet only
+    at the barriers around the timed region and for the max of their times."""
+
     def __init__(self):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = os.environ.get("MAYO_BENCH_DIST_BACKEND", "nccl")
         self.pg = None
         if self.world > 1:
             import datetime
 
             import torch.distributed as dist
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            dist.init_process_group(self.backend, timeout=datetime.timedelta(seconds=120))
             self.pg = dist
 
     def barrier(self):
         if self.pg:
-            import torch
-            self.pg.barrier(device_ids=[self.local])
-            torch.cuda.synchronize()
+            if self.backend == "nccl":
+                import torch
+                self.pg.barrier(device_ids=[self.local])
+                torch.cuda.synchronize()
+            else:
+                self.pg.barrier()
 
     def max(self, x: float) -> float:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device="cuda" if self.backend == "nccl" else "cpu")
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
+
+
+def weak_value(ops_per_rank_step: float, world: int, ms_per_step_max: float) -> float:
+    """Whole-job throughput under weak scaling: every rank processes its own batch, so the job
+    did world x the per-rank operations in the slowest rank's time."""
+    return ops_per_rank_step * world / (ms_per_step_max / 1e3)
 
 
 class Clocks:
@@ -583,7 +597,7 @@ def run_ours(args, dist: Dist):
     bad_e2e = int((h_res.numpy() != expected).sum())
 
     ms_per_step = total_ms / args.steps
-    value = ops_per_step * dist.world / (ms_per_step / 1e3)
+    value = weak_value(ops_per_step, dist.world, ms_per_step)
     sm_mhz = clk.get("sm_mhz") or 1965.0
     peak_ops = LOP3_LANE_OPS_PER_CLK_SM * 148 * sm_mhz * 1e6 / 1e9  # G lane-ops/s
     dom = max(phase_ms, key=phase_ms.get)
