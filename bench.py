@@ -271,7 +271,8 @@ def run_ours(args, dist: Dist):
         res = torch.zeros(batch, dtype=torch.uint8, device=dev)
         h_sig = torch.zeros(batch * z.sig_bytes, dtype=torch.uint8).pin_memory()
         h_res = torch.zeros(batch, dtype=torch.uint8).pin_memory()
-        launches_per_step = 7  # sign: hash, key tiles, tensor-core product, tail; verify: the last three
+        # per call: hashing order (count, scatter), hash, key tiles, tensor-core product, tail, fix-up
+        launches_per_step = 14
 
         def sign_op():
             m.sign_shared(esk, d_msgs, sig, ws, batch, msg_off=d_offs, msg_len=d_lens, stream=st)

@@ -24,6 +24,8 @@
 //                       gather bit 7 of 32 sums into one word -- one 32-coordinate bit plane -- and
 //                       store the planes.  Zero blocks of A (columns c < r of the triangular P1 / P)
 //                       are skipped.  Waits are bounded: a timeout sets the status word and unwinds.
+//   Messages of different lengths: hash_order_count/scatter_kernel first group the instances by
+//   SHAKE256 block count, and the hash kernels take them in that order.
 //   sign: sign_hash_kernel (thread per instance) -> product -> sign_shared_tail_kernel (first
 //         attempt from the planes in a compact CTA) -> sign_shared_fix_kernel (retries of the
 //         rare singular first attempts with the engine).
@@ -49,6 +51,7 @@ constexpr int SH_ISSUE_WARP = SH_EPI_NT / 32;       // warps 8, 9: MMA issuers (
 constexpr int SH_LOAD_WARP = SH_ISSUE_WARP + 2;     // warp 10: key loader
 constexpr int SH_GEMM_NT = SH_EPI_NT + 96;
 constexpr int SH_FIX_CTAS = 2 * 148;
+constexpr int ORD_CTAS = 64, ORD_NT = 256, ORD_BINS = 8;  // hashing-order sort: grid cap, threads, bins
 
 // The product for sign (rows: T_j[r] over P1 for r < v, then M_j[b] over L) or verify (rows
 // T_j[r] over [[P1, P2], [0, P3]] for r < n).
@@ -130,13 +133,82 @@ struct SharedWs {
     static constexpr size_t inst = VERIFY ? pad16((size_t)NW * 4) : pad16(SignWs<SET>::total);
     static constexpr size_t planes = P::PLANES * 16;
     static constexpr size_t retry = VERIFY ? 0 : 4;
-    static constexpr size_t head = a + a_bytes + op_bytes;
-    static size_t bytes(size_t batch) { return head + batch * (inst + planes + retry); }
+    static constexpr size_t order = 4;  // hashing order (instances grouped by message blocks)
+    static constexpr size_t hist_bytes = (size_t)ORD_CTAS * ORD_BINS * 4;
+    static constexpr size_t head = a + a_bytes + op_bytes + hist_bytes;
+    static size_t bytes(size_t batch) { return head + batch * (inst + planes + retry + order); }
     static size_t op_off() { return a + a_bytes; }
+    static size_t hist_off() { return a + a_bytes + op_bytes; }
     static size_t inst_off() { return head; }
     static size_t planes_off(size_t batch) { return head + batch * inst; }
     static size_t retry_off(size_t batch) { return head + batch * (inst + planes); }
+    static size_t order_off(size_t batch) { return head + batch * (inst + planes + retry); }
 };
+
+// ---- hashing order ----
+// The hash kernels run one instance per thread, and a warp runs as many Keccak-f permutations as
+// its longest message needs.  With lengths that differ per instance, a counting sort by the
+// number of SHAKE256 blocks of the message (capped at ORD_BINS - 1 full blocks) lets each warp
+// hash messages of one size class.  Each instance's outputs go to its own workspace row, so the
+// order changes no byte.  Two launches: per-CTA bin counts over a contiguous chunk, then a
+// scatter from each (bin, CTA) start.
+__device__ __forceinline__ uint32_t msg_bin(const MsgIO &m, uint32_t i) {
+    const uint32_t b = m.len(i) / 136;
+    return b < (uint32_t)ORD_BINS - 1 ? b : (uint32_t)ORD_BINS - 1;
+}
+__device__ __forceinline__ void ord_chunk(uint32_t batch, uint32_t &b0, uint32_t &b1) {
+    const uint32_t per = (batch + gridDim.x - 1) / gridDim.x;
+    b0 = blockIdx.x * per;
+    b1 = b0 + per < batch ? b0 + per : batch;
+}
+__global__ void __launch_bounds__(ORD_NT) hash_order_count_kernel(const MsgIO m, uint32_t batch, uint32_t *hist) {
+    __shared__ uint32_t h[ORD_BINS];
+    if (threadIdx.x < ORD_BINS) h[threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t b0, b1;
+    ord_chunk(batch, b0, b1);
+    for (uint32_t i = b0 + threadIdx.x; i < b1; i += ORD_NT) atomicAdd(&h[msg_bin(m, i)], 1u);
+    __syncthreads();
+    if (threadIdx.x < ORD_BINS) hist[blockIdx.x * ORD_BINS + threadIdx.x] = h[threadIdx.x];
+}
+__global__ void __launch_bounds__(ORD_NT)
+    hash_order_scatter_kernel(const MsgIO m, uint32_t batch, const uint32_t *hist, uint32_t *order) {
+    __shared__ uint32_t cur[ORD_BINS];
+    if (threadIdx.x < 32) {  // start of (bin t, this CTA): every lower bin, then bin t of earlier CTAs
+        uint32_t acc[ORD_BINS];
+#pragma unroll
+        for (int t = 0; t < ORD_BINS; t++) acc[t] = 0;
+        for (uint32_t c = threadIdx.x; c < gridDim.x; c += 32)
+#pragma unroll
+            for (int b = 0; b < ORD_BINS; b++) {
+                const uint32_t v = hist[c * ORD_BINS + b];
+#pragma unroll
+                for (int t = 0; t < ORD_BINS; t++) acc[t] += (b < t || (b == t && c < blockIdx.x)) ? v : 0u;
+            }
+#pragma unroll
+        for (int t = 0; t < ORD_BINS; t++) {
+            const uint32_t tot = __reduce_add_sync(0xffffffffu, acc[t]);
+            if (threadIdx.x == 0) cur[t] = tot;
+        }
+    }
+    __syncthreads();
+    uint32_t b0, b1;
+    ord_chunk(batch, b0, b1);
+    for (uint32_t i = b0 + threadIdx.x; i < b1; i += ORD_NT) order[atomicAdd(&cur[msg_bin(m, i)], 1u)] = i;
+}
+// The order for a call, or nullptr when every message has the same length (nothing to group).
+template <int SET, bool VERIFY>
+static const uint32_t *launch_hash_order(const MsgIO &m, uint8_t *ws, size_t batch, cudaStream_t st) {
+    using WSL = SharedWs<SET, VERIFY>;
+    if (!m.msg_len || batch < 2 * (size_t)HASH_NT) return nullptr;
+    const size_t want = (batch + ORD_NT - 1) / ORD_NT;
+    const unsigned g = (unsigned)(want < (size_t)ORD_CTAS ? want : (size_t)ORD_CTAS);
+    uint32_t *hist = reinterpret_cast<uint32_t *>(ws + WSL::hist_off());
+    uint32_t *order = reinterpret_cast<uint32_t *>(ws + WSL::order_off(batch));
+    hash_order_count_kernel<<<g, ORD_NT, 0, st>>>(m, (uint32_t)batch, hist);
+    hash_order_scatter_kernel<<<g, ORD_NT, 0, st>>>(m, (uint32_t)batch, hist, order);
+    return order;
+}
 
 // A, tiled: group gi = rr * W + w holds rows rho = 32 b + q (bit plane b; row q carries coordinate
 // 32 w + cq(q), cq(q) = 8 ((q >> 2) & 3) + 2 (q & 3) + (q >> 4), the order in which the epilogue's
@@ -491,10 +563,12 @@ __global__ void __launch_bounds__(SignCfg<SET>::NT)
 // ---- verify ----
 // Thread per instance: digest = SHAKE256(M), t = SHAKE256(digest || salt) (src/verify.cu:37-48).
 template <int SET>
-__global__ void verify_hash_kernel(const VerifyIO io, uint8_t *tws, size_t tws_stride, uint32_t batch) {
+__global__ void verify_hash_kernel(const VerifyIO io, uint8_t *tws, size_t tws_stride, uint32_t batch,
+                                   const uint32_t *order) {
     using S = Set<SET>;
-    const uint32_t inst = blockIdx.x * blockDim.x + threadIdx.x;
-    if (inst >= batch) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= batch) return;
+    const uint32_t inst = order ? order[i] : i;  // order: instances grouped by message blocks
     alignas(8) uint8_t digest[S::digest];
     Sponge<136> sp;
     sp.init();
@@ -659,7 +733,8 @@ static int sign_shared_t(const SignIO &io0, uint8_t *ws, size_t batch, cudaStrea
     io.ws_stride = WSL::inst;
     tl_tm.n = 0;
     tmark(st);
-    int rc = launch_sign_hash(SET, io, batch, st);
+    const uint32_t *order = launch_hash_order<SET, false>(io.m, ws, batch, st);
+    int rc = launch_sign_hash(SET, io, batch, st, order);
     tmark(st);
     if (rc != ST_OK) return rc;
     rc = launch_product<SET, false>(io.esk, io.ws + SignWs<SET>::vr, io.ws_stride, ws, batch, st);
@@ -689,8 +764,9 @@ static int verify_shared_t(const VerifyIO &io0, uint8_t *ws, size_t batch, cudaS
     uint8_t *tws = ws + WSL::inst_off();
     tl_tm.n = 0;
     tmark(st);
+    const uint32_t *order = launch_hash_order<SET, true>(io.m, ws, batch, st);
     verify_hash_kernel<SET><<<(unsigned)((batch + HASH_NT - 1) / HASH_NT), HASH_NT, 0, st>>>(io, tws, WSL::inst,
-                                                                                       (uint32_t)batch);
+                                                                                       (uint32_t)batch, order);
     tmark(st);
     int rc = launch_product<SET, true>(io.epk, io.sig, io.sig_stride, ws, batch, st);
     if (rc != ST_OK) return rc;

@@ -9,11 +9,12 @@
 namespace mayo {
 
 template <int SET>
-__global__ void sign_hash_kernel(const SignIO io, uint32_t batch) {
+__global__ void sign_hash_kernel(const SignIO io, uint32_t batch, const uint32_t *order) {
     using S = Set<SET>;
     using WS = SignWs<SET>;
-    const uint32_t inst = blockIdx.x * blockDim.x + threadIdx.x;
-    if (inst >= batch) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= batch) return;
+    const uint32_t inst = order ? order[i] : i;  // order: instances grouped by message blocks
     const uint8_t *seed_sk = io.esk + (size_t)inst * io.esk_stride;
     uint8_t *ws = io.ws + (size_t)inst * io.ws_stride;
     alignas(8) uint8_t digest[S::digest];
@@ -83,20 +84,21 @@ __global__ void __launch_bounds__(SignCfg<SET>::NT) sign_kernel(const SignIO io)
 template <int SET>
 static int sign_t(const SignIO &io, size_t batch, cudaStream_t st) {
     using C = SignCfg<SET>;
-    sign_hash_kernel<SET><<<(unsigned)((batch + HASH_NT - 1) / HASH_NT), HASH_NT, 0, st>>>(io, (uint32_t)batch);
+    sign_hash_kernel<SET><<<(unsigned)((batch + HASH_NT - 1) / HASH_NT), HASH_NT, 0, st>>>(io, (uint32_t)batch, nullptr);
     if (!set_smem_attr(sign_kernel<SET>, C::total)) return ST_CUDA;
     sign_kernel<SET><<<(unsigned)batch, C::NT, C::total, st>>>(io);
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
 }
 
-int launch_sign_hash(int set, const SignIO &io, size_t batch, cudaStream_t st) {
+int launch_sign_hash(int set, const SignIO &io, size_t batch, cudaStream_t st, const uint32_t *order) {
     if (batch == 0) return ST_OK;
     const unsigned g = (unsigned)((batch + HASH_NT - 1) / HASH_NT);
+    const uint32_t b = (uint32_t)batch;
     switch (set) {
-        case 1: sign_hash_kernel<1><<<g, HASH_NT, 0, st>>>(io, (uint32_t)batch); break;
-        case 2: sign_hash_kernel<2><<<g, HASH_NT, 0, st>>>(io, (uint32_t)batch); break;
-        case 3: sign_hash_kernel<3><<<g, HASH_NT, 0, st>>>(io, (uint32_t)batch); break;
-        case 5: sign_hash_kernel<5><<<g, HASH_NT, 0, st>>>(io, (uint32_t)batch); break;
+        case 1: sign_hash_kernel<1><<<g, HASH_NT, 0, st>>>(io, b, order); break;
+        case 2: sign_hash_kernel<2><<<g, HASH_NT, 0, st>>>(io, b, order); break;
+        case 3: sign_hash_kernel<3><<<g, HASH_NT, 0, st>>>(io, b, order); break;
+        case 5: sign_hash_kernel<5><<<g, HASH_NT, 0, st>>>(io, b, order); break;
         default: return ST_BAD_SET;
     }
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;

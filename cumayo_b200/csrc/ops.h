@@ -72,7 +72,8 @@ struct VerifyIO {
 };
 int launch_sign_io(int set, const SignIO &io, size_t batch, cudaStream_t st);
 // Only the hash stage of sign (digest, salt, t, V || r for ctr 0 into io.ws).
-int launch_sign_hash(int set, const SignIO &io, size_t batch, cudaStream_t st);
+// order (optional, batch entries): thread i hashes instance order[i]
+int launch_sign_hash(int set, const SignIO &io, size_t batch, cudaStream_t st, const uint32_t *order = nullptr);
 int launch_verify_io(int set, const VerifyIO &io, size_t batch, cudaStream_t st);
 // Workspace bytes per instance used by sign (digest, salt, t, V || r).
 size_t sign_ws_bytes(int set);
