@@ -350,7 +350,10 @@ class Mayo:
                           esk_stride=0, sig_stride=None, stream=None):
         """sign_many without a caller workspace, for callers that cannot allocate device memory:
         the workspace is a fixed array inside the library (batch <= sign_noalloc_max_batch()).
-        Calls must not overlap on the GPU; the first call on a device must precede stream capture."""
+        Calls must not overlap on the GPU.  The first call on a device (and the first after the
+        device's context is replaced, e.g. by a device reset) looks up the array's address; make
+        it outside stream capture: made during a capture it may fail with MayoError (status
+        MAYO_B200_ERR_CUDA)."""
         z = self.sizes
         rc = lib().mayo_b200_sign_many_noalloc(self.set, _ptr(esk), esk_stride, _ptr(msgs), _ptr(msg_off),
                                                _ptr(msg_len), msg_stride, mlen, _ptr(sig),

@@ -10,11 +10,29 @@
 #include "common.cuh"
 #include "ops.h"
 
+namespace mayo {
+
+thread_local int g_last_cuda_error = 0;
+
+int api_cuda_rc(cudaError_t e) {
+    if (e == cudaSuccess) return MAYO_B200_OK;
+    g_last_cuda_error = (int)e;
+    return MAYO_B200_ERR_CUDA;
+}
+
+int api_launch_rc(int rc) {
+    // cudaGetLastError also clears the error a failed launch left, so the next call's
+    // cudaPeekAtLastError reports only its own launches
+    if (rc == ST_CUDA) g_last_cuda_error = (int)cudaGetLastError();
+    return rc;
+}
+
+}  // namespace mayo
+
 namespace {
 
 using namespace mayo;
 
-thread_local int g_last_cuda_error = 0;
 
 struct Sz {
     size_t sk, pk, sig, esk, epk, p, o_bytes, scratch;
@@ -39,15 +57,8 @@ bool sizes_of(int set, Sz &z) {
 inline size_t A(size_t x) { return align128z(x); }
 inline cudaStream_t S_(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
-int cuda_rc(cudaError_t e) {
-    if (e == cudaSuccess) return MAYO_B200_OK;
-    g_last_cuda_error = (int)e;
-    return MAYO_B200_ERR_CUDA;
-}
-int kernel_rc(int rc) {
-    if (rc == ST_CUDA) g_last_cuda_error = (int)cudaGetLastError();
-    return rc;
-}
+int cuda_rc(cudaError_t e) { return mayo::api_cuda_rc(e); }
+int kernel_rc(int rc) { return mayo::api_launch_rc(rc); }
 
 // Row sizes of each reference entry point (tests/bench_stream.cu:25-31, 82, 133 of the reference).
 size_t row_keypair(const Sz &z) { return A(z.sk) + A(z.pk) + A(z.p); }
@@ -124,7 +135,7 @@ MAYO_B200_API const char *mayo_b200_status_string(int status) {
     }
 }
 
-MAYO_B200_API int mayo_b200_last_cuda_error(void) { return g_last_cuda_error; }
+MAYO_B200_API int mayo_b200_last_cuda_error(void) { return mayo::g_last_cuda_error; }
 
 // ---- keypair (src/api.cu:17-38) ----
 MAYO_B200_API int mayo_b200_keypair(int set, uint8_t *pool, size_t pitch, size_t batch, void *stream,

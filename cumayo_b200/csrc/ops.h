@@ -84,4 +84,10 @@ int launch_verify_shared(int set, const VerifyIO &io, uint8_t *ws, size_t batch,
 int shared_timing(int enable);
 int shared_timing_read(float *ms);
 
+// Status plumbing of the C-ABI (capi.cu): a failed CUDA call or launch is recorded as the calling
+// thread's last CUDA error (mayo_b200_last_cuda_error) and reported as ST_CUDA.  api_launch_rc
+// takes a launcher's status and, for ST_CUDA, reads and clears the runtime's last error.
+int api_cuda_rc(cudaError_t e);
+int api_launch_rc(int rc);
+
 }  // namespace mayo

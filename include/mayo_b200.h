@@ -308,9 +308,12 @@ MAYO_B200_API int mayo_b200_serve_unpack(const mayo_b200_serve_req *req, uint32_
  * arguments and results as mayo_b200_sign_many minus `ws`: the workspace is a 4 MiB array
  * compiled into the library, held by every GPU that loads the library until exit.  Batches
  * above mayo_b200_sign_noalloc_max_batch(set) return MAYO_B200_ERR_TOO_LARGE.  The first call
- * on a device looks up the array's address on that device: make it before any stream
- * capture.  All calls share the array, so calls whose GPU work may overlap (different streams
- * without ordering) race and must not be issued.  Allocates nothing. */
+ * on a device looks up the array's address on that device and keeps it for the device's
+ * current CUDA context; a call in a new context of the device (after cudaDeviceReset, for
+ * instance) looks it up again.  Make the first call before any stream capture: the look-up is
+ * not a stream operation, and a first call made while a stream is being captured may fail with
+ * MAYO_B200_ERR_CUDA.  All calls share the array, so calls whose GPU work may overlap
+ * (different streams without ordering) race and must not be issued.  Allocates nothing. */
 MAYO_B200_API size_t mayo_b200_sign_noalloc_max_batch(int set);
 MAYO_B200_API int mayo_b200_sign_many_noalloc(int set, const uint8_t *esk, size_t esk_stride, const uint8_t *msgs,
                                               const uint64_t *msg_off, const uint32_t *msg_len, size_t msg_stride,

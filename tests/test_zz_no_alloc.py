@@ -48,6 +48,34 @@ def test_noalloc_matches_sign_many_twice(s, cuda):
         assert torch.equal(got, want)
 
 
+def test_noalloc_full_array_matches_sign_many_and_oracle(cuda):
+    """MAYO_5 at exactly mayo_b200_sign_noalloc_max_batch instances: the last instance's
+    workspace ends at the end of the fixed array."""
+    import torch
+    from oracle import oracle as O
+    s = 5
+    m = Mayo(s)
+    z = m.sizes
+    batch = m.sign_noalloc_max_batch()
+    assert batch * m.sign_ws_bytes() <= 4 << 20 < (batch + 1) * m.sign_ws_bytes()
+    rng = np.random.default_rng(5151)
+    seed = rng.integers(0, 256, z.sk_bytes, dtype=np.uint8).tobytes()
+    esk_h = np.frombuffer(O.expandsk(s, seed), np.uint8)
+    esk = torch.from_numpy(esk_h.copy()).cuda()
+    msgs, offs, lens = _inputs(m, rng, batch)
+    got = torch.full((batch * z.sig_bytes,), 0xAB, dtype=torch.uint8, device="cuda")
+    m.sign_many_noalloc(esk, msgs, got, batch, msg_off=offs, msg_len=lens)
+    ws = torch.zeros(batch * m.sign_ws_bytes(), dtype=torch.uint8, device="cuda")
+    want = torch.zeros_like(got)
+    m.sign_many(esk, msgs, want, ws, batch, msg_off=offs, msg_len=lens)
+    torch.cuda.synchronize()
+    assert torch.equal(got, want)
+    body, o_h, l_h = msgs.cpu().numpy(), offs.cpu().numpy().view(np.uint64), lens.cpu().numpy().view(np.uint32)
+    ml = [body[int(a):int(a) + int(n)].tobytes() for a, n in zip(o_h, l_h)]
+    osig, _ = O.sign_batch(s, esk_h[None, :], ml, shared_key=True)
+    assert np.array_equal(got.cpu().numpy().reshape(batch, z.sig_bytes), osig)
+
+
 def test_noalloc_rejects_batch_above_limit(cuda):
     import torch
     m = Mayo(3)
