@@ -452,45 +452,12 @@ def run_ours(args, dist: Dist):
     elif wl["kind"] == "distinct_verify":
         # every instance has its own keypair; epk resident in the verify pool, 10% corrupted sigs
         mlen = wl["mlen"][0]
-        seeds = seeds_for(seed, batch, z.sk_bytes)
-        msgs = chacha((b"mayo-b200-msgs-%d" % seed).ljust(32, b"\0")[:32], batch * mlen).reshape(batch, mlen)
-        vpool, vp = m.alloc_pool("verify", batch, mlen)
-        V2 = vpool.view(batch, vp)
-        msg_v = A128(z.epk_bytes)
-        sig_v = msg_v + A128(mlen)
-        res_off = sig_v + A128(z.sig_bytes)
-        chunk = 2048  # set-up in chunks: keypair pools are large for MAYO_5
-        for c0 in range(0, batch, chunk):
-            nb = min(chunk, batch - c0)
-            kpool, kp = m.alloc_pool("keypair", nb)
-            K2 = kpool.view(nb, kp)
-            K2[:, : z.sk_bytes].copy_(torch.from_numpy(seeds[c0:c0 + nb]))
-            m.crypto_sign_keypair_from_seed(kpool, kp, nb, st)
-            pk_off = A128(z.sk_bytes)
-            V2[c0:c0 + nb, z.p_bytes - 16: z.p_bytes - 16 + z.pk_bytes].copy_(K2[:, pk_off: pk_off + z.pk_bytes])
-            spool, spch = m.alloc_pool("signWithesk", nb, mlen)
-            S2 = spool.view(nb, spch)
-            S2[:, : z.sk_bytes].copy_(K2[:, : z.sk_bytes])
-            ms_ = A128(z.esk_bytes)
-            S2[:, ms_: ms_ + mlen].copy_(torch.from_numpy(msgs[c0:c0 + nb]))
-            m.crypto_sign_signWithesk(spool, mlen, spch, nb, st)
-            ss_ = ms_ + A128(mlen)
-            V2[c0:c0 + nb, sig_v: sig_v + z.sig_bytes].copy_(S2[:, ss_: ss_ + z.sig_bytes])
-            del kpool, spool
-        m.crypto_sign_expandpk(vpool, vp, batch, st)
-        V2[:, msg_v: msg_v + mlen].copy_(torch.from_numpy(msgs))
-        torch.cuda.synchronize()
-        good_sigs = V2[:, sig_v: sig_v + z.sig_bytes].cpu().numpy()
-        rng = np.random.default_rng(seed)
-        bad_idx = np.sort(rng.choice(batch, batch // 10, replace=False))
-        sigs = good_sigs.copy()
-        for i in bad_idx:
-            pos = int(rng.integers(0, 2 * z.sig_bytes))
-            sigs[i, pos // 2] ^= np.uint8(int(rng.integers(1, 16)) << (4 * (pos % 2)))
+        dv = build_distinct_verify(m, batch, seed, mlen, st)
+        vpool, vp, V2, msgs, sigs, bad_idx = dv["vpool"], dv["pitch"], dv["rows"], dv["msgs"], dv["sigs"], dv["bad"]
+        msg_v, sig_v, res_off = dv["msg_off"], dv["sig_off"], dv["res_off"]
         h_sig = torch.from_numpy(sigs).pin_memory()
         h_msgs = torch.from_numpy(msgs.copy()).pin_memory()
         h_res = torch.zeros(batch, dtype=torch.uint8).pin_memory()
-        V2[:, sig_v: sig_v + z.sig_bytes].copy_(h_sig)
         launches_per_step = 1
 
         def verify_op():
@@ -692,6 +659,61 @@ def run_ours(args, dist: Dist):
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
     return out
+
+
+def corrupt_tenth(sigs: np.ndarray, seed: int):
+    """A seeded tenth of the signatures get one uniformly random nibble flipped (nonzero XOR)."""
+    batch, sb = sigs.shape
+    rng = np.random.default_rng(seed)
+    bad_idx = np.sort(rng.choice(batch, batch // 10, replace=False))
+    out = sigs.copy()
+    for i in bad_idx:
+        pos = int(rng.integers(0, 2 * sb))
+        out[i, pos // 2] ^= np.uint8(int(rng.integers(1, 16)) << (4 * (pos % 2)))
+    return out, bad_idx
+
+
+def build_distinct_verify(m, batch: int, seed: int, mlen: int, st):
+    """C3 inputs on the device: `batch` ChaCha20-seeded keypairs, each signing its own `mlen`-byte
+    message (pool API), expanded public keys resident in a verify pool (the reference's verify
+    layout), then a seeded tenth of the signatures corrupted.  Returns the pool and host copies."""
+    import torch
+    z = m.sizes
+    seeds = seeds_for(seed, batch, z.sk_bytes)
+    msgs = chacha((b"mayo-b200-msgs-%d" % seed).ljust(32, b"\0")[:32], batch * mlen).reshape(batch, mlen)
+    vpool, vp = m.alloc_pool("verify", batch, mlen)
+    V2 = vpool.view(batch, vp)
+    msg_v = A128(z.epk_bytes)
+    sig_v = msg_v + A128(mlen)
+    res_off = sig_v + A128(z.sig_bytes)
+    pks = np.zeros((batch, z.pk_bytes), np.uint8)
+    chunk = 2048  # set-up in chunks: keypair pools are large for MAYO_5
+    for c0 in range(0, batch, chunk):
+        nb = min(chunk, batch - c0)
+        kpool, kp = m.alloc_pool("keypair", nb)
+        K2 = kpool.view(nb, kp)
+        K2[:, : z.sk_bytes].copy_(torch.from_numpy(seeds[c0:c0 + nb]))
+        m.crypto_sign_keypair_from_seed(kpool, kp, nb, st)
+        pk_off = A128(z.sk_bytes)
+        V2[c0:c0 + nb, z.p_bytes - 16: z.p_bytes - 16 + z.pk_bytes].copy_(K2[:, pk_off: pk_off + z.pk_bytes])
+        pks[c0:c0 + nb] = K2[:, pk_off: pk_off + z.pk_bytes].cpu().numpy()
+        spool, spch = m.alloc_pool("signWithesk", nb, mlen)
+        S2 = spool.view(nb, spch)
+        S2[:, : z.sk_bytes].copy_(K2[:, : z.sk_bytes])
+        ms_ = A128(z.esk_bytes)
+        S2[:, ms_: ms_ + mlen].copy_(torch.from_numpy(msgs[c0:c0 + nb]))
+        m.crypto_sign_signWithesk(spool, mlen, spch, nb, st)
+        ss_ = ms_ + A128(mlen)
+        V2[c0:c0 + nb, sig_v: sig_v + z.sig_bytes].copy_(S2[:, ss_: ss_ + z.sig_bytes])
+        del kpool, spool
+    m.crypto_sign_expandpk(vpool, vp, batch, st)
+    V2[:, msg_v: msg_v + mlen].copy_(torch.from_numpy(msgs))
+    torch.cuda.synchronize()
+    good_sigs = V2[:, sig_v: sig_v + z.sig_bytes].cpu().numpy()
+    sigs, bad_idx = corrupt_tenth(good_sigs, seed)
+    V2[:, sig_v: sig_v + z.sig_bytes].copy_(torch.from_numpy(sigs))
+    return dict(vpool=vpool, pitch=vp, rows=V2, seeds=seeds, msgs=msgs, pks=pks, good_sigs=good_sigs, sigs=sigs,
+                bad=bad_idx, msg_off=msg_v, sig_off=sig_v, res_off=res_off)
 
 
 def expand_shared_key(m, key_seed: np.ndarray, dev, st):
@@ -1359,13 +1381,13 @@ def main():
                     help="c2: sub-batches (one stream each) of the end-to-end measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--int-peak", action="store_true",
-                    help="build and run cumayo_b200/peaks/int_pipes.cu (integer-pipe rates) and exit")
+                    help="build and run bench_int_pipes.cu (integer-pipe rates) and exit")
     args = ap.parse_args()
     if args.int_peak:
         from cumayo_b200.build import ARCH, BUILD, nvcc
         os.makedirs(BUILD, exist_ok=True)
         exe = os.path.join(BUILD, "int_pipes")
-        subprocess.run([nvcc()] + ARCH + ["-O3", "-o", exe, os.path.join(ROOT, "cumayo_b200", "peaks", "int_pipes.cu")],
+        subprocess.run([nvcc()] + ARCH + ["-O3", "-o", exe, os.path.join(ROOT, "bench_int_pipes.cu")],
                        check=True)
         subprocess.run([exe], check=True)
         return

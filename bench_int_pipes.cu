@@ -1,4 +1,4 @@
-// int_pipes.cu -- integer-pipe throughput of the GPU (warp-instructions per SM-cycle) for LOP3, IMAD,
+// bench_int_pipes.cu -- integer-pipe throughput of the GPU (warp-instructions per SM-cycle) for LOP3, IMAD,
 // SHF, PRMT, IADD, a LOP3+IMAD mix, shared-memory loads and shuffles.  bench.py uses the LOP3 rate
 // as the peak of its integer-ALU roofline (`python bench.py --int-peak` builds and runs this file).
 // Every access is in bounds by construction: one output word per thread, a 4 KB shared buffer

@@ -105,8 +105,22 @@ def lib() -> ctypes.CDLL:
         L.mayo_b200_shared_timing.argtypes = [ctypes.c_int]
         L.mayo_b200_shared_timing_read.restype = ctypes.c_int
         L.mayo_b200_shared_timing_read.argtypes = [ctypes.POINTER(ctypes.c_float)]
+        L.mayo_b200_test_inject.restype = ctypes.c_int
+        L.mayo_b200_test_inject.argtypes = [ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32]
         _lib = L
     return _lib
+
+
+INJECT_NONE, INJECT_QUEUE_LOST_PUSH, INJECT_PRODUCT_STALL = 0, 1, 2
+
+
+def test_inject(kind: int, arg: int = 0, spin: int = 0) -> None:
+    """Failure injection for tests (mayo_b200_test_inject), for calls from this thread:
+    INJECT_QUEUE_LOST_PUSH gives every queue bucket a slot nothing publishes, so its bounded
+    wait runs out (MAYO_B200_QUEUE_ERR_TIMEOUT); INJECT_PRODUCT_STALL stops the tensor-core
+    product's key loader after `arg` chunks with waits of `spin` polls (the status word becomes
+    1 and the per-instance engine computes the results); INJECT_NONE turns it off."""
+    _check(lib().mayo_b200_test_inject(kind, arg, spin), "test_inject")
 
 
 def _check(rc: int, what: str) -> None:

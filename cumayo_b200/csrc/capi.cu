@@ -27,6 +27,9 @@ int api_launch_rc(int rc) {
     return rc;
 }
 
+thread_local Inject tl_inject;
+Inject &inject() { return tl_inject; }
+
 }  // namespace mayo
 
 namespace {
@@ -136,6 +139,12 @@ MAYO_B200_API const char *mayo_b200_status_string(int status) {
 }
 
 MAYO_B200_API int mayo_b200_last_cuda_error(void) { return mayo::g_last_cuda_error; }
+
+MAYO_B200_API int mayo_b200_test_inject(int kind, uint32_t arg, uint32_t spin) {
+    if (kind < MAYO_B200_INJECT_NONE || kind > MAYO_B200_INJECT_PRODUCT_STALL) return MAYO_B200_ERR_ARG;
+    mayo::inject() = mayo::Inject{kind, arg, spin};
+    return MAYO_B200_OK;
+}
 
 // ---- keypair (src/api.cu:17-38) ----
 MAYO_B200_API int mayo_b200_keypair(int set, uint8_t *pool, size_t pitch, size_t batch, void *stream,

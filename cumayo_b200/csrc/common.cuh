@@ -534,28 +534,20 @@ __host__ __device__ constexpr uint64_t gf16_inv_table() {
     return t;
 }
 constexpr uint64_t kGf16InvTable = gf16_inv_table();
-// Division table: byte 16 p + e = e / p (e times the inverse of p; row p = 0 all zero), four bytes
-// per word, little-endian.
-struct Gf16DivTable {
-    uint32_t w[64];
-};
-__host__ __device__ constexpr Gf16DivTable gf16_div_table() {
-    Gf16DivTable t{};
-    for (uint32_t p = 0; p < 16; p++) {
-        uint32_t inv = 0;
-        for (uint32_t b = 1; b < 16; b++)
-            if (gf16_mul_cx(p, b) == 1) inv = b;
-        for (uint32_t e = 0; e < 16; e++) {
-            const uint32_t i = 16 * p + e;
-            t.w[i >> 2] |= gf16_mul_cx(e, inv) << (8 * (i & 3));
-        }
-    }
-    return t;
-}
-constexpr Gf16DivTable kGf16Div = gf16_div_table();
-__constant__ Gf16DivTable c_gf16_div = kGf16Div;
 __host__ __device__ __forceinline__ uint32_t gf16_inv_reg(uint32_t a) {
     return (uint32_t)(kGf16InvTable >> (4 * (a & 0xF))) & 0xFu;
+}
+// x * b in GF(16) (x^4 = x + 1), without branches.
+__host__ __device__ __forceinline__ uint32_t gf16_xtime(uint32_t b) {
+    return ((b << 1) & 0xFu) ^ ((0u - (b >> 3)) & 0x3u);
+}
+// Quotient e / a from the basis multiples B_s = a^-1 x^s (s = 0..3) and the bits e_s of e:
+// e / a = sum_s e_s B_s.  The bits come as words that are zero or not; masks select the B_s, so
+// the quotient costs no memory access and no branch on e or a.
+__host__ __device__ __forceinline__ uint32_t gf16_div_from_basis(uint32_t e0, uint32_t e1, uint32_t e2, uint32_t e3,
+                                                                const uint4 &B) {
+    return ((0u - (uint32_t)(e0 != 0u)) & B.x) ^ ((0u - (uint32_t)(e1 != 0u)) & B.y) ^
+           ((0u - (uint32_t)(e2 != 0u)) & B.z) ^ ((0u - (uint32_t)(e3 != 0u)) & B.w);
 }
 
 // Multiply the eight packed nibbles of a word by a public constant c (0..15).

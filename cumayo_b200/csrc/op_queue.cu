@@ -288,12 +288,13 @@ __global__ void queue_fill_kernel(uint32_t *slots, size_t nslots, uint32_t *ctrl
 // warp ballots give each item's rank within its warp and bucket, a scan over the warps gives the
 // warp's offset).  Items of a bucket without a kernel (`active` bit clear) are dropped with an
 // operand error in that bucket's control words, items with op 3 likewise in block 12.  n_dev,
-// when given, lowers n.
+// when given, lowers n.  `phantom` (failure injection for tests) raises the tail of every bucket
+// with items by one slot that stays empty, as if a push had been lost.
 constexpr int Q_PART_NT = 1024;
 __global__ void __launch_bounds__(Q_PART_NT) queue_partition_kernel(const uint32_t *items, uint32_t n,
                                                                     const uint32_t *n_dev, uint32_t *slots,
                                                                     uint32_t capacity, uint32_t *ctrl,
-                                                                    uint32_t active) {
+                                                                    uint32_t active, uint32_t phantom) {
     __shared__ uint32_t s_warp[Q_PART_NT / 32][Q_BUCKETS + 1];
     __shared__ uint32_t s_base[Q_BUCKETS + 1];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -339,7 +340,8 @@ __global__ void __launch_bounds__(Q_PART_NT) queue_partition_kernel(const uint32
             c[0] = cnt;  // dropped
             if (cnt) c[3] = MAYO_B200_QUEUE_ERR_OPERAND;
         } else {
-            c[1] = cnt < capacity ? cnt : capacity;
+            const uint32_t t = cnt + (cnt && phantom ? 1u : 0u);
+            c[1] = t < capacity ? t : capacity;
             if (cnt > capacity) c[3] = MAYO_B200_QUEUE_ERR_FULL;
         }
     }
@@ -532,7 +534,9 @@ MAYO_B200_API int mayo_b200_queue_run(const mayo_b200_queue_ops ops[4], const ui
 
     const size_t fill_n = nslots > (size_t)mayo::Q_CTRL_TOTAL ? nslots : (size_t)mayo::Q_CTRL_TOTAL;
     mayo::queue_fill_kernel<<<(unsigned)((fill_n + 255) / 256), 256, 0, st>>>(slots, nslots, ctrl);
-    mayo::queue_partition_kernel<<<1, mayo::Q_PART_NT, 0, st>>>(items, n, n_device, slots, cap_words, ctrl, active);
+    const uint32_t phantom = mayo::inject().kind == MAYO_B200_INJECT_QUEUE_LOST_PUSH ? 1u : 0u;
+    mayo::queue_partition_kernel<<<1, mayo::Q_PART_NT, 0, st>>>(items, n, n_device, slots, cap_words, ctrl, active,
+                                                                phantom);
     if (cudaPeekAtLastError() != cudaSuccess || cudaEventRecord(fs->fork, st) != cudaSuccess) return MAYO_B200_ERR_CUDA;
     int k = 0;
     for (int j = 0; j < Q_BUCKETS; j++) {

@@ -266,6 +266,16 @@ __device__ __forceinline__ uint32_t pack_bit7x32(const uint32_t (&r)[16]) {
     return x;
 }
 
+// Bounded wait on an mbarrier phase that also gives up as soon as another warp of the CTA has
+// recorded a failure in *fail (checked every 64 polls).
+__device__ __forceinline__ bool wait_or_fail(uint64_t *bar, uint32_t parity, uint32_t limit, const uint32_t *fail) {
+    for (uint32_t i = 0; i < limit; i += 64) {
+        if (tc::mbar_wait(bar, parity, 64)) return true;
+        if (*reinterpret_cast<const volatile uint32_t *>(fail)) return false;
+    }
+    return false;
+}
+
 // vec: instance i's vectors start at vec + i * vec_stride, entry c of vector j is nibble
 // j * NVEC + c.  planes: instance i at planes + i * PLANES, [j][row][w].
 //
@@ -282,10 +292,15 @@ __device__ __forceinline__ uint32_t pack_bit7x32(const uint32_t (&r)[16]) {
 // (copy landed), empty[chunk] (commit: its MMAs completed), mma_done[acc] (commit), acc_free[acc]
 // (8 arrivals), drain[issuer] (an issuer's last commit).  The loader starts as soon as the
 // barriers exist; the others first build the vector columns.
+//
+// `spin` bounds the waits of the steady state (polls); the unwind waits keep SH_SPIN.
+// `stall_after` is failure injection for tests: the loader silently stops after that many
+// chunks, so the issuers' waits for the next chunk run out (0xFFFFFFFF: never).
 template <int SET, bool VERIFY>
 __global__ void __launch_bounds__(SH_GEMM_NT, 1)
     shared_gemm_kernel(const uint8_t *__restrict__ A, const uint8_t *__restrict__ vec, size_t vec_stride,
-                       uint4 *__restrict__ planes, uint32_t batch, uint32_t *ctl) {
+                       uint4 *__restrict__ planes, uint32_t batch, uint32_t *ctl, uint32_t spin,
+                       uint32_t stall_after) {
     using P = SharedProb<SET, VERIFY>;
     using S = Set<SET>;
     constexpr int NIN = P::NINST, KPAD = P::KPAD, NT = P::NTILES, NB = P::NB, G = P::G;
@@ -342,16 +357,20 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
         // ---------------- loader: chunk c (k-steps a .. a + n - 1 of one tile) -> slot c % NCH ----------------
         if (lane == 0) {
             uint32_t c = 0;
-            bool ok = true;
+            bool ok = true, stalled = false;
 #pragma unroll 1
-            for (int i = 0; i < NT && ok; i++) {
+            for (int i = 0; i < NT && ok && !stalled; i++) {
                 const int t = tile_of(i);
                 const uint8_t *src = A + (size_t)t * P::TILE;
 #pragma unroll 1
                 for (int a = first_step(t); a < P::KSTEPS; a += (int)CK, c++) {
                     const uint32_t cs = c % NCH;
+                    if (c >= stall_after) {  // failure injection: stop without telling the other warps
+                        stalled = true;
+                        break;
+                    }
                     if (*reinterpret_cast<volatile uint32_t *>(s_fail) ||
-                        (c >= NCH && !tc::mbar_wait(&empty[cs], (c / NCH - 1) & 1u, SH_SPIN))) {
+                        (c >= NCH && !wait_or_fail(&empty[cs], (c / NCH - 1) & 1u, spin, s_fail))) {
                         ok = false;
                         break;
                     }
@@ -414,7 +433,7 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
                     continue;
                 }
                 const int b = i & 1;
-                if (i >= 2 && !tc::mbar_wait(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, SH_SPIN)) {
+                if (i >= 2 && !wait_or_fail(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, spin, s_fail)) {
                     ok = false;
                     break;
                 }
@@ -426,11 +445,11 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
                     // The other issuer's tile may hold unloaded chunks older than c, so slot cs
                     // can still be a phase behind chunk c: a parity wait is only meaningful once
                     // the loader has armed chunk c's phase.
-                    uint32_t spin = 0;
-                    while (*reinterpret_cast<volatile uint32_t *>(s_loaded) <= c && ++spin < SH_SPIN) {
+                    uint32_t polls = 0;
+                    while (*reinterpret_cast<volatile uint32_t *>(s_loaded) <= c && ++polls < spin) {
                     }
                     __threadfence_block();
-                    if (spin >= SH_SPIN || !tc::mbar_wait(&full[cs], (c / NCH) & 1u, SH_SPIN)) {
+                    if (polls >= spin || !tc::mbar_wait(&full[cs], (c / NCH) & 1u, spin)) {
                         ok = false;
                         break;
                     }
@@ -479,7 +498,7 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
 #pragma unroll 1
         for (int i = 0; i < NT; i++) {
             const int b = i & 1;
-            if (!tc::mbar_wait(&mma_done[b], (uint32_t)(i >> 1) & 1u, SH_SPIN)) {
+            if (!wait_or_fail(&mma_done[b], (uint32_t)(i >> 1) & 1u, spin, s_fail)) {
                 atomicOr(s_fail, 1u);
                 break;
             }
@@ -714,8 +733,11 @@ static int launch_product(const uint8_t *key, const uint8_t *vec, size_t vec_str
     tmark(st);
     if (!set_smem_attr(shared_gemm_kernel<SET, VERIFY>, P::SMEM)) return ST_CUDA;
     uint4 *planes = reinterpret_cast<uint4 *>(ws + WSL::planes_off(batch));
+    const Inject &inj = inject();
+    const bool stall = inj.kind == MAYO_B200_INJECT_PRODUCT_STALL;
+    const uint32_t spin = stall && inj.spin ? inj.spin : SH_SPIN;
     shared_gemm_kernel<SET, VERIFY><<<(unsigned)((batch + P::NI - 1) / P::NI), SH_GEMM_NT, P::SMEM, st>>>(
-        A, vec, vec_stride, planes, (uint32_t)batch, ctl);
+        A, vec, vec_stride, planes, (uint32_t)batch, ctl, spin, stall ? inj.arg : 0xFFFFFFFFu);
     tmark(st);
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
 }

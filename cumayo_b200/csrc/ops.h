@@ -90,4 +90,11 @@ int shared_timing_read(float *ms);
 int api_cuda_rc(cudaError_t e);
 int api_launch_rc(int rc);
 
+// Failure injection for tests (mayo_b200_test_inject), per host thread; kind 0 = off.
+struct Inject {
+    int kind = 0;
+    uint32_t arg = 0, spin = 0;
+};
+Inject &inject();
+
 }  // namespace mayo

@@ -5,10 +5,11 @@
 //   M_i = V_i L                                  engine over the columns of L (sign.cu:256-330)
 //   A = sum z^l M                                packed z-shifts, one thread per column (sign.cu:333-393)
 //   x = solve(A, y, r)                           Gauss-Jordan over bit-planes, no data branches (sign.cu:10-145)
-// No branch depends on a value derived from the secret key; only the attempt count is data
-// dependent, as in MAYO.  One shared-memory read depends on the data: the elimination's
-// 256-byte division table at index (a_p, e); the reference's elimination (sign.cu:48-100)
-// branches on the entries and reads its multiplication table the same way.
+// No branch and no memory address depends on a value derived from the secret key; only the
+// attempt count is data dependent, as in MAYO.  In the elimination the pivot's inverse comes
+// from a shift of a 64-bit register constant and each column's factor from mask arithmetic
+// (gf16_div_from_basis), where the reference's elimination (sign.cu:48-100) branches on the
+// entries and indexes its multiplication and inverse tables with them.
 //
 // Why the elimination may differ from the reference's and still give identical bytes: when
 // rank A = m, the reference's pivot columns are the lexicographically first column basis of A
@@ -57,7 +58,7 @@ struct SignCfg {
     static constexpr size_t off_upk = X_IN_BS ? off_bs + (sz_bs > sz_acol ? sz_bs : sz_acol) : off_x + sz_x;
     static constexpr size_t off_mpk = off_upk + pad16((size_t)S::pairs * NW * 4);
     static constexpr size_t off_piv = off_mpk + pad16((size_t)S::k * S::o * NW * 4);
-    static constexpr size_t off_rhs = off_piv + (size_t)2 * (W + 2) * 16;
+    static constexpr size_t off_rhs = off_piv + (size_t)2 * (W + 3) * 16;
     static constexpr size_t off_y = off_rhs + (size_t)W * 16;
     static constexpr size_t off_key = off_y + pad16(NW * 4);
     static constexpr size_t off_t = off_key + pad16(S::digest + 2 * S::sk + 1);
@@ -137,7 +138,7 @@ __device__ __forceinline__ void sign_load_ws(uint8_t *smem, int tid, const uint8
     uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
     uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
     uint32_t *mpk = reinterpret_cast<uint32_t *>(smem + C::off_mpk);  // [k][o][NW]
-    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W + 3]
     uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);     // [W]
     uint32_t *ypk = reinterpret_cast<uint32_t *>(smem + C::off_y);
     uint8_t *s_key = smem + C::off_key;  // digest || salt || seed_sk || ctr
@@ -186,7 +187,7 @@ __device__ __forceinline__ void sign_hash_cta(uint8_t *smem, int tid, const uint
     uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
     uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
     uint32_t *mpk = reinterpret_cast<uint32_t *>(smem + C::off_mpk);  // [k][o][NW]
-    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W + 3]
     uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);     // [W]
     uint32_t *ypk = reinterpret_cast<uint32_t *>(smem + C::off_y);
     uint8_t *s_key = smem + C::off_key;  // digest || salt || seed_sk || ctr
@@ -227,7 +228,7 @@ __device__ __forceinline__ void sign_next_vr(uint8_t *smem, int tid, int ctr) {
     uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
     uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
     uint32_t *mpk = reinterpret_cast<uint32_t *>(smem + C::off_mpk);  // [k][o][NW]
-    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W + 3]
     uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);     // [W]
     uint32_t *ypk = reinterpret_cast<uint32_t *>(smem + C::off_y);
     uint8_t *s_key = smem + C::off_key;  // digest || salt || seed_sk || ctr
@@ -261,7 +262,7 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
     uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
     uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
     uint32_t *mpk = reinterpret_cast<uint32_t *>(smem + C::off_mpk);  // [k][o][NW]
-    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W + 3]
     uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);     // [W]
     uint32_t *ypk = reinterpret_cast<uint32_t *>(smem + C::off_y);
     uint8_t *s_key = smem + C::off_key;  // digest || salt || seed_sk || ctr
@@ -473,10 +474,6 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
         }
     }
     for (int i = tid; i < W * 4; i += NT) reinterpret_cast<uint32_t *>(rhsacc)[i] = 0;
-    // the division table for the elimination, in the V-mask area (free once M is formed)
-    uint8_t *s_div = reinterpret_cast<uint8_t *>(masks);
-    static_assert((size_t)S::v * J * 16 >= 256, "division table fits the mask area");
-    for (int i = tid; i < 64; i += NT) reinterpret_cast<uint32_t *>(s_div)[i] = c_gf16_div.w[i];
     __syncthreads();
 
     // ---- Gauss-Jordan without data branches.  Thread owns columns c = KO - (tid + NT q): the RHS on
@@ -524,11 +521,13 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
         for (int w = 0; w < W; w++) my_oh[q][w] = 0;
     }
     // The owner of a column computes its pivot (lowest unpivoted row with a nonzero entry) a_p and
-    // publishes D = a + e_p, the row one-hot and a_p in buffer pcx & 1; a column with entry e in
-    // row p then takes col ^= (e / a_p) D, which is col ^= e F' with F' = a_p^-1 (a + e_p).
+    // publishes D = a + e_p, the row one-hot and the basis multiples B_s = a_p^-1 x^s in buffer
+    // pcx & 1 ([0, W) D, [W, W + 2) one-hot words, [W + 2] B); a column with entry e in row p
+    // then takes col ^= (e / a_p) D with e / a_p = sum_s e_s B_s, which is col ^= e F' with
+    // F' = a_p^-1 (a + e_p).
     auto publish = [&](int q, int pcx) {
-        uint4 *buf = pivbuf + (pcx & 1) * (W + 2);
-        uint32_t *ohw = reinterpret_cast<uint32_t *>(buf + W);  // oh[0..W), found at [7]
+        uint4 *buf = pivbuf + (pcx & 1) * (W + 3);
+        uint32_t *ohw = reinterpret_cast<uint32_t *>(buf + W);  // oh[0..W)
         uint32_t oh[W], found = 0;
 #pragma unroll
         for (int w = 0; w < W; w++) {
@@ -557,7 +556,9 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
             ohw[w] = oh[w];
             my_oh[q][w] = oh[w];
         }
-        ohw[7] = piv;
+        // a_p^-1 by a shift of a register constant, then x a_p^-1, x^2 a_p^-1, x^3 a_p^-1
+        const uint32_t b0 = gf16_inv_reg(piv), b1 = gf16_xtime(b0), b2 = gf16_xtime(b1), b3 = gf16_xtime(b2);
+        buf[W + 2] = make_uint4(b0, b1, b2, b3);
         my_has[q] = found;
     };
 #pragma unroll
@@ -576,7 +577,7 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
         // be a no-op; skipping it depends only on the public loop index.  Lookahead: the owner
         // of column pc + 1 publishes its pivot right after its own update, while the other
         // columns update, so each step needs one barrier and the owner's chain overlaps them.
-        const uint4 *buf = pivbuf + (pc & 1) * (W + 2);
+        const uint4 *buf = pivbuf + (pc & 1) * (W + 3);
         const uint32_t *ohw = reinterpret_cast<const uint32_t *>(buf + W);
         G4 D[W];
         uint32_t oh[W];
@@ -586,7 +587,7 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
             oh[w] = ohw[w];
             pivoted[w] |= oh[w];
         }
-        const uint8_t *drow = s_div + 16 * ohw[7];  // e / a_p
+        const uint4 Bp = buf[W + 2];  // a_p^-1 x^s, s = 0..3
 #pragma unroll
         for (int q = 0; q < CPT; q++) {
             const int c = KO - (tid + NT * q);
@@ -599,9 +600,7 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
                 e2 |= col[q][w].p2 & oh[w];
                 e3 |= col[q][w].p3 & oh[w];
             }
-            const uint32_t e = (uint32_t)(e0 != 0) | ((uint32_t)(e1 != 0) << 1) | ((uint32_t)(e2 != 0) << 2) |
-                               ((uint32_t)(e3 != 0) << 3);
-            const uint4 fm = scalar_masks(drow[e]);
+            const uint4 fm = scalar_masks(gf16_div_from_basis(e0, e1, e2, e3, Bp));  // e / a_p
 #pragma unroll
             for (int w = 0; w < W; w++) g4_madd(col[q][w], D[w], fm);
             if (c == pc + 1 && c < KO) publish(q, c);
@@ -680,7 +679,7 @@ __device__ __forceinline__ void sign_write(uint8_t *smem, int tid, const uint8_t
     uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
     uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
     uint32_t *mpk = reinterpret_cast<uint32_t *>(smem + C::off_mpk);  // [k][o][NW]
-    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W + 3]
     uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);     // [W]
     uint32_t *ypk = reinterpret_cast<uint32_t *>(smem + C::off_y);
     uint8_t *s_key = smem + C::off_key;  // digest || salt || seed_sk || ctr

@@ -68,6 +68,28 @@ MAYO_B200_API const char *mayo_b200_status_string(int status);
 /* Last cudaError_t seen by this library on the calling thread (0 = none). */
 MAYO_B200_API int mayo_b200_last_cuda_error(void);
 
+/* ---- Failure injection for tests (no counterpart in the reference: its kernels have no
+ * waits and no error path, src/sign.cu:244-474) ----
+ * Makes one of the library's bounded device waits run out on purpose, so a test can check that
+ * the error is reported, that nothing hangs or faults and that the results stay right.  The
+ * setting belongs to the calling host thread and applies to its later calls until it is
+ * changed; MAYO_B200_INJECT_NONE (the default) turns it off.
+ *   MAYO_B200_INJECT_QUEUE_LOST_PUSH: in mayo_b200_queue_run every bucket with items gets one
+ *     slot past its items that nothing publishes (as if a push were lost).  The CTA that takes
+ *     that slot waits `spin_limit` sleeps, records MAYO_B200_QUEUE_ERR_TIMEOUT in the bucket's
+ *     control words and ends; every real item is still processed.  (arg, spin unused.)
+ *   MAYO_B200_INJECT_PRODUCT_STALL: in mayo_b200_sign_shared / _verify_shared the key loader of
+ *     each tensor-core product CTA stops after `arg` chunks without telling the other warps,
+ *     and the product's waits give up after `spin` polls (0 = the default bound).  The product
+ *     then sets its status word to 1 and the per-instance engine computes every result.
+ * MAYO_B200_ERR_ARG for an unknown kind. */
+enum {
+    MAYO_B200_INJECT_NONE = 0,
+    MAYO_B200_INJECT_QUEUE_LOST_PUSH = 1,
+    MAYO_B200_INJECT_PRODUCT_STALL = 2
+};
+MAYO_B200_API int mayo_b200_test_inject(int kind, uint32_t arg, uint32_t spin);
+
 /* ---- keypair: reference src/api.cu:17-38 ---- */
 /* Instance b uses seed_sk = SHAKE128(LE64(rand_index + 2b + 1)).  Row: sk @0, pk @A128(SK),
  * P1||P2 scratch @A128(SK)+A128(PK). */

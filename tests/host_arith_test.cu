@@ -27,11 +27,17 @@ int main() {
         if (gf16_inv_reg(a) != gf16_inv_ct(a)) FAIL("gf16_inv_reg %u", a);
     }
     if (gf16_inv_ct(0) != 0) FAIL("inv(0)");
-    for (uint32_t p = 0; p < 16; p++)  // division table of the elimination: byte 16 p + e = e / p
+    for (uint32_t p = 0; p < 16; p++) {  // the elimination's quotient e / p from the basis multiples
+        const uint32_t b0 = gf16_inv_reg(p), b1 = gf16_xtime(b0), b2 = gf16_xtime(b1), b3 = gf16_xtime(b2);
+        const uint4 B = make_uint4(b0, b1, b2, b3);
         for (uint32_t e = 0; e < 16; e++) {
-            const uint32_t i = 16 * p + e, d = (kGf16Div.w[i >> 2] >> (8 * (i & 3))) & 0xFF;
+            // entry bits as words that are zero or not (any set bit counts), as the columns hold them
+            const uint32_t sh = rnd() & 31;
+            const uint32_t d = gf16_div_from_basis((e & 1) << sh, ((e >> 1) & 1) << sh, ((e >> 2) & 1) << sh,
+                                                   ((e >> 3) & 1) << sh, B);
             if (p == 0 ? d != 0 : ref_mul(d, p) != e) FAIL("gf16 div %u / %u", e, p);
         }
+    }
     for (int it = 0; it < 2000; it++) {
         uint32_t w[4] = {rnd(), rnd(), rnd(), rnd()}, s = rnd() & 0xF;
         // packed -> planes: plane bit b holds coordinate 8*(b&3) + (b>>2)
