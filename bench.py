@@ -22,6 +22,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -81,6 +82,10 @@ VERIFY_TRAFFIC_PER_INST = {3: (1.557413e9 + 4.978176e6) / 4096, 5: (3.478466e9 +
 WORKLOADS = {
     "c2": dict(set=2, batch=65536, kind="shared_sign_verify", mlen=(32, 1024)),
     "c1": dict(set=1, batch=1024, kind="keypair_sign_verify", mlen=(32, 32)),
+    # the same keypair -> sign -> verify batch for the other sets (per-set figures)
+    "c1-2": dict(set=2, batch=1024, kind="keypair_sign_verify", mlen=(32, 32)),
+    "c1-3": dict(set=3, batch=1024, kind="keypair_sign_verify", mlen=(32, 32)),
+    "c1-5": dict(set=5, batch=1024, kind="keypair_sign_verify", mlen=(32, 32)),
     "c3-3": dict(set=3, batch=16384, kind="distinct_verify", mlen=(32, 32)),
     "c3-5": dict(set=5, batch=16384, kind="distinct_verify", mlen=(32, 32)),
     "c4": dict(set=0, batch=262144, kind="mixed_queue", mlen=(32, 32)),
@@ -243,6 +248,7 @@ def run_ours(args, dist: Dist):
     device_streamed_step = None
     plain_api = "per-(set, op) batched launches: keypair_from_seed, sign_many, verify_many"
     plain_check = None
+    gpu_outputs = None  # host copies of the last end-to-end step's outputs, for the oracle check
 
     if wl["kind"] == "shared_sign_verify":
         # one resident expanded key (esk, epk), messages of per-instance length
@@ -302,6 +308,9 @@ def run_ours(args, dist: Dist):
         def d2h():
             h_sig.copy_(sig, non_blocking=True)
             h_res.copy_(res, non_blocking=True)
+
+        def gpu_outputs():
+            return {"sig": h_sig.numpy().reshape(batch, z.sig_bytes), "res": h_res.numpy()}
 
         # End to end: the batch in `e2e_chunks` sub-batches on as many streams (the reference
         # benchmark's pattern), so one sub-batch's copies overlap another's kernels.  Each
@@ -433,6 +442,9 @@ def run_ours(args, dist: Dist):
             h_sig.copy_(S2[:, sig_s: sig_s + z.sig_bytes], non_blocking=True)
             h_res.copy_(V2[:, res_off], non_blocking=True)
 
+        def gpu_outputs():
+            return {"pk": h_pk.numpy(), "sig": h_sig.numpy(), "res": h_res.numpy()}
+
         h2d_bytes = seeds.nbytes + 2 * msgs.nbytes
         d2h_bytes = batch * (z.pk_bytes + z.sig_bytes + 1)
         phases = [("keypair", keypair_op), ("sign", sign_op), ("verify", verify_op)]
@@ -443,7 +455,7 @@ def run_ours(args, dist: Dist):
                 "verify": macs["verify"] * batch}
         hbm_bytes = {"keypair": 2 * batch * z.p_bytes, "sign": 3 * batch * z.esk_bytes,
                      "verify": 2 * batch * z.epk_bytes}
-        cfg = {"workload": "MAYO_1 keypair -> sign -> verify, distinct keys", "set": f"MAYO_{s}", "batch": batch,
+        cfg = {"workload": f"MAYO_{s} keypair -> sign -> verify, distinct keys", "set": f"MAYO_{s}", "batch": batch,
                "msg_len": f"{mlen} B", "key": "per-instance seeded keypairs (ChaCha20)",
                "l2": "flushed between steps (256 MiB write)",
                "api": "crypto_sign_keypair_from_seed / signWithesk / verifyWithepk (pool API)"}
@@ -469,6 +481,9 @@ def run_ours(args, dist: Dist):
 
         def d2h():
             h_res.copy_(V2[:, res_off], non_blocking=True)
+
+        def gpu_outputs():
+            return {"pk": dv["pks"], "good_sig": dv["good_sigs"], "sig_in": sigs, "res": h_res.numpy()}
 
         h2d_bytes = msgs.nbytes + sigs.nbytes
         d2h_bytes = batch
@@ -656,8 +671,42 @@ def run_ours(args, dist: Dist):
                         "api": plain_api}
         if plain_check is not None:
             out["result_mismatches"] += plain_check()
+    if wl["kind"] == "shared_sign_verify" and dist.world == 1 and getattr(args, "per_set", False):
+        per = per_set_measure(args, dist, run_ours)
+        m2 = per.setdefault(f"MAYO_{s}", {"mismatches": 0})
+        m2["shared_key_batch"] = batch
+        m2["shared_sign_per_s"] = out["sign_per_s"]
+        m2["shared_verify_per_s"] = out["verify_per_s"]
+        # the reference arm of this bench, when it ran on this GPU shortly before, leaves its
+        # per-set figures in REF_PER_SET_FILE: add them and the ratios
+        ref = None
+        try:
+            with open(REF_PER_SET_FILE) as f:
+                ref = json.load(f)
+            if ref.get("gpu") != gpu_identity(dist.local) or time.time() - float(ref.get("time", 0)) > 6 * 3600:
+                ref = None
+        except (OSError, ValueError):
+            ref = None
+        for key, ent in per.items():
+            out["result_mismatches"] += ent["mismatches"]
+            r = (ref or {}).get("per_set", {}).get(key)
+            if r:
+                ent["reference"] = {k: v for k, v in r.items() if k.endswith("_per_s")}
+                ent["vs_reference"] = {k: round(ent[k] / v, 2) for k, v in ent["reference"].items()
+                                       if k in ent and v}
+        out["per_set"] = per
+        out["per_set_note"] = ("ops/s, device-timed (CUDA events), L2 flushed between steps: keypair/sign/verify = "
+                               "keypair_from_seed / signWithesk / verifyWithepk at batch 1,024 with distinct keys and "
+                               "32-byte messages (the reference benchmark's operations); distinct_verify = "
+                               "crypto_sign_verify at 16,384 (C3); shared = this line's MAYO_2 shared-key run. "
+                               "'reference' = the reference's own build on this GPU, from this bench's reference arm "
+                               + ("run at " + time.strftime("%Y-%m-%d %H:%M:%S", time.gmtime(float(ref["time"])))
+                                  + " UTC" if ref else "(not run on this GPU: no ratio)"))
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(args)
+        cb = cpu_baseline(args, gpu_outputs() if gpu_outputs is not None else None)
+        out["cpu_baseline"] = cb
+        if cb is not None and cb.get("oracle_check") is not None:
+            out["result_mismatches"] += cb["oracle_check"]["mismatches"]
     return out
 
 
@@ -839,14 +888,67 @@ def setup_mixed_queue(args, dist, batch, seed, st):
 
 
 # ---------------------------------------------------------------------------------------------
+# per-set figures: keypair / sign / verify of every parameter set (the reference benchmark's three
+# operations, tests/bench_stream.cu:47-176 of the reference) and the distinct-key verifies
+# ---------------------------------------------------------------------------------------------
+PER_SET_RUNS = ("c1", "c1-2", "c1-3", "c1-5", "c3-3", "c3-5")
+REF_PER_SET_FILE = os.path.join(tempfile.gettempdir(), "mayo_b200_reference_per_set.json")
+
+
+def per_set_measure(args, dist, runner) -> dict:
+    """Runs the per-set workloads with `runner` (run_ours or run_reference) and collects ops/s per
+    set: keypair/sign/verify at batch 1,024 (distinct keys, 32-byte messages) and, for MAYO_3/5,
+    the distinct-key verify at 16,384."""
+    per = {}
+    for name in PER_SET_RUNS:
+        sub = argparse.Namespace(**vars(args))
+        sub.workload, sub.batch, sub.no_cpu_baseline, sub.per_set = name, 0, True, False
+        sub.steps, sub.warmup = min(args.steps, 10), max(3, min(args.warmup, 3))
+        r = runner(sub, dist)
+        wl = WORKLOADS[name]
+        ent = per.setdefault(f"MAYO_{wl['set']}", {"mismatches": 0})
+        ph = r.get("phase_ms", {})
+        if wl["kind"] == "keypair_sign_verify":
+            ent["batch"] = wl["batch"]
+            for op in ("keypair", "sign", "verify"):
+                if op in ph and ph[op] > 0:
+                    ent[f"{op}_per_s"] = round(wl["batch"] / (ph[op] / 1e3), 1)
+        else:
+            ent["distinct_verify_batch"] = wl["batch"]
+            if ph.get("verify", 0) > 0:
+                ent["distinct_verify_per_s"] = round(wl["batch"] / (ph["verify"] / 1e3), 1)
+        ent["mismatches"] += int(r.get("result_mismatches", 0))
+    return per
+
+
+def gpu_identity(dev_index: int) -> str:
+    import torch
+    p = torch.cuda.get_device_properties(dev_index)
+    return f"{p.name}/{getattr(p, 'uuid', '')}"
+
+
+# ---------------------------------------------------------------------------------------------
 # CPU baseline: the oracle (a restatement of the reference's algorithm) on the host cores
 # ---------------------------------------------------------------------------------------------
-def cpu_baseline(args, sample: int | None = None):
+def cpu_baseline(args, gpu: dict | None = None, sample: int | None = None):
+    """The oracle timed on the host cores on a bounded sample of the workload: the first `sample`
+    instances of rank 0's own inputs (the ChaCha20 generators give the same prefix).  Its outputs
+    for those instances are also compared byte for byte with the GPU's (`gpu`: host copies of the
+    last end-to-end step), reported as `oracle_check`."""
     from oracle import oracle as O
     wl = WORKLOADS[args.workload]
     s = wl["set"]
     P = O.params(s)
     threads = O.max_threads()
+
+    def check(pairs, n):
+        if gpu is None:
+            return None
+        bad = 0
+        for name, want, got in pairs:
+            bad += int((np.asarray(want) != np.asarray(got)).reshape(n, -1).any(axis=1).sum())
+        return {"instances": n, "compared": [p[0] for p in pairs], "mismatches": bad}
+
     if wl["kind"] == "shared_sign_verify":
         sample = sample or 4096
         seed = seeds_for(1, 1, P.sk_bytes)[0].tobytes()
@@ -862,10 +964,13 @@ def cpu_baseline(args, sample: int | None = None):
         res = O.verify_batch(s, epk, msgs, sig, shared_key=True)
         t_ver = time.perf_counter() - t
         assert int(res.sum()) == 0
+        n = min(sample, gpu["sig"].shape[0]) if gpu else 0
         return {"value": round(2 * sample / (t_sign + t_ver), 1), "unit": "ops/s", "cores": threads, "kind": "port",
                 "sample": f"{sample} signs + {sample} verifies of the same workload (shared MAYO_2 key, "
                           f"32..1024 B messages), OpenMP one instance per thread",
-                "sign_per_s": round(sample / t_sign, 1), "verify_per_s": round(sample / t_ver, 1)}
+                "sign_per_s": round(sample / t_sign, 1), "verify_per_s": round(sample / t_ver, 1),
+                "oracle_check": check([("signature", sig[:n], gpu["sig"][:n]), ("verify byte", res[:n], gpu["res"][:n])],
+                                      n) if gpu else None}
     if wl["kind"] == "keypair_sign_verify":
         sample = sample or 4 * wl["batch"]
         seeds = seeds_for(1, sample, P.sk_bytes)
@@ -880,11 +985,14 @@ def cpu_baseline(args, sample: int | None = None):
         res = O.verify_batch(s, O.expandpk_batch(s, pk), [bytes(x) for x in msgs], sig)
         t_ver = time.perf_counter() - t
         assert int(res.sum()) == 0
+        n = min(sample, gpu["sig"].shape[0]) if gpu else 0
         return {"value": round(3 * sample / (t_kp + t_sign + t_ver), 1), "unit": "ops/s", "cores": threads,
                 "kind": "port", "sample": f"{sample} instances of keypair -> sign (expand-sk inside) -> verify "
                                           f"(expand-pk inside), MAYO_{s}, OpenMP one instance per thread",
                 "keypair_per_s": round(sample / t_kp, 1), "sign_per_s": round(sample / t_sign, 1),
-                "verify_per_s": round(sample / t_ver, 1)}
+                "verify_per_s": round(sample / t_ver, 1),
+                "oracle_check": check([("public key", pk[:n], gpu["pk"][:n]), ("signature", sig[:n], gpu["sig"][:n]),
+                                       ("verify byte", res[:n], gpu["res"][:n])], n) if gpu else None}
     if wl["kind"] == "distinct_verify":
         sample = sample or (512 if s == 5 else 1024)
         seeds = seeds_for(1, sample, P.sk_bytes)
@@ -892,13 +1000,19 @@ def cpu_baseline(args, sample: int | None = None):
         pk = O.keypair_from_seed_batch(s, seeds)
         sig, _ = O.sign_batch(s, O.expandsk_batch(s, seeds), msgs)
         epk = O.expandpk_batch(s, pk)
+        # the GPU's own verify inputs (a tenth corrupted) when given, else the clean signatures
+        vin = gpu["sig_in"][:sample] if gpu else sig
         t = time.perf_counter()
-        res = O.verify_batch(s, epk, msgs, sig)
+        res = O.verify_batch(s, epk, msgs, vin)
         t_ver = time.perf_counter() - t
-        assert int(res.sum()) == 0
+        if gpu is None:
+            assert int(res.sum()) == 0
         return {"value": round(sample / t_ver, 1), "unit": "ops/s", "cores": threads, "kind": "port",
                 "sample": f"{sample} distinct-key verifies (expanded keys precomputed), MAYO_{s}, OpenMP one "
-                          f"instance per thread"}
+                          f"instance per thread",
+                "oracle_check": check([("public key", pk, gpu["pk"][:sample]),
+                                       ("signature", sig, gpu["good_sig"][:sample]),
+                                       ("verify byte", res, gpu["res"][:sample])], sample) if gpu else None}
     return None
 
 
@@ -1013,6 +1127,20 @@ def run_reference(args, dist: Dist):
         bad += int(vpool[r0:r0 + cnt, ro].sum().item())
     ms = dist.max((sum(ts) + sum(tv)) / args.steps)
     value = 2 * batch * dist.world / (ms / 1e3)
+    per = None
+    if dist.world == 1 and getattr(args, "per_set", False):
+        del spool, vpool
+        torch.cuda.empty_cache()
+        per = per_set_measure(args, dist, run_reference)
+        m2 = per.setdefault(f"MAYO_{s}", {"mismatches": 0})
+        m2["shared_key_batch"] = batch
+        m2["shared_sign_per_s"] = round(batch / (sum(ts) / len(ts) / 1e3), 1)
+        m2["shared_verify_per_s"] = round(batch / (sum(tv) / len(tv) / 1e3), 1)
+        try:
+            with open(REF_PER_SET_FILE, "w") as f:
+                json.dump({"time": time.time(), "gpu": gpu_identity(dist.local), "per_set": per}, f)
+        except OSError:
+            pass
     return {"metric": METRIC, "value": round(value, 1), "unit": "ops/s", "impl": "reference", "n_gpus": dist.world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded ChaCha20)",
@@ -1023,7 +1151,7 @@ def run_reference(args, dist: Dist):
                               "round-robin over 10 streams (the reference benchmark's stream pattern)"},
             "sign_per_s": round(batch * dist.world / (sum(ts) / len(ts) / 1e3), 1),
             "verify_per_s": round(batch * dist.world / (sum(tv) / len(tv) / 1e3), 1),
-            "launches_per_step": 2 * len(groups), "rejected_valid_signatures": bad,
+            "launches_per_step": 2 * len(groups), "rejected_valid_signatures": bad, "per_set": per,
             "cpu_baseline": {"value": round(value, 1), "unit": "ops/s", "cores": 0, "kind": "reference",
                              "sample": "not a CPU run: the reference has no CPU implementation; this arm times "
                                        "its own CUDA build on the same B200"},
@@ -1380,6 +1508,8 @@ def main():
     ap.add_argument("--e2e-chunks", type=int, default=8,
                     help="c2: sub-batches (one stream each) of the end-to-end measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-per-set", dest="per_set", action="store_false",
+                    help="skip the per-set keypair/sign/verify and distinct-key verify figures (default run)")
     ap.add_argument("--int-peak", action="store_true",
                     help="build and run bench_int_pipes.cu (integer-pipe rates) and exit")
     args = ap.parse_args()
