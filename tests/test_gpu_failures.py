@@ -112,7 +112,9 @@ def test_queue_full_drops_requeued_sign(cuda):
     torch.cuda.synchronize()
     p = q.stats()["per_bucket"][(s, Q.OP_SIGN)]
     assert p["error"] == Q.QUEUE_ERR_FULL
-    assert p["requeued_signs"] == 0 and p["finished"] == n  # the dropped item counts as finished
+    # the push that found no slot raised the tail and counts as finished, so the bucket drains
+    # (finished == tail): n items + the dropped second attempt
+    assert p["requeued_signs"] == 0 and p["finished"] == p["published"] == n + 1
     got = ops.sg_sig.cpu().numpy().reshape(n, z.sig_bytes)
     want, att = O.sign_batch(s, np.stack([esk] * n), [m.tobytes() for m in msgs])
     assert att[r] == 2 and (att[np.arange(n) != r] == 1).all()
