@@ -1330,12 +1330,12 @@ def run_serving(args, dist: Dist):
 
     # keys (all resident: 4096 keys ~ 2 GB of esk + epk, far inside the budget)
     seeds = {s: seeds_for(seed * 100 + s, SERVE_KEYS[s], M.sizes(s).sk_bytes) for s in sets}
-    cache = SV.KeyCache(seeds, SV.KeyCache.capacity_for_budget(budget // 2, SERVE_KEYS), device=dev)
-    server = SV.Server(cache, max_batch=max_batch, inflight=args.inflight, max_msg=max_msg, budget_bytes=budget)
+    key_slots = SV.capacity_for_budget(budget // 2, SERVE_KEYS)
+    server = SV.Server(seeds, key_slots=key_slots, max_batch=max_batch, inflight=args.inflight, max_msg=max_msg,
+                       budget_bytes=budget, device=dev)
     for s in sets:  # load every key once, outside the timed runs
-        _, su = cache.acquire(s, np.arange(SERVE_KEYS[s]), st)
-        cache.release(s, su)
-    torch.cuda.synchronize()
+        server.preload(s, np.arange(SERVE_KEYS[s]))
+    key_cache_bytes = sum(key_slots[s] * (M.sizes(s).esk_bytes + M.sizes(s).epk_bytes) for s in sets)
 
     # request templates: per set 4096 (key, message) pairs and their signatures, computed by the
     # server itself; a sample is checked against the plain batched sign_many below
@@ -1362,52 +1362,61 @@ def run_serving(args, dist: Dist):
         rows = np.arange(lo, min(T, lo + max_batch), dtype=np.uint64)
         r = SV.make_requests(np.full(rows.size, Q.OP_SIGN, np.uint8), tset[rows], tkey[rows], tmlen[rows],
                              tmsg.ctypes.data + rows * ROW_MSG, 0, tsig.ctypes.data + rows * ROW_SIG)
-        server.launch(r, tag=(lo, lo + rows.size))
+        server.submit(r, lo)
         server.drain()
     server.check_queue()
     tbad = tsig.copy()
     tbad[:, 7] ^= 0x40  # every template's signature, corrupted
-    # cross-check: 64 templates per set through the plain batched path (gathered keys)
+    # cross-check: 64 templates per set through the plain batched path (keys expanded by the pool API)
     plain_bad = 0
     for s in sets:
         z = M.sizes(s)
+        m_ = M.Mayo(s)
         rows = tmpl_base[s] + np.arange(64)
-        esk = cache.esk[s].view(-1, z.esk_bytes)[torch.from_numpy(cache.tables[s].slot_of[tkey[rows]]).to(dev)]
+        kp, kpitch = m_.alloc_pool("keypair", 64)
+        kp.view(64, kpitch)[:, : z.sk_bytes].copy_(torch.from_numpy(seeds[s][tkey[rows]]))
+        m_.crypto_sign_keypair_from_seed(kp, kpitch, 64, st)
+        esk = torch.zeros(64 * z.esk_bytes, dtype=torch.uint8, device=dev)
+        esk.view(64, z.esk_bytes)[:, : z.sk_bytes].copy_(kp.view(64, kpitch)[:, : z.sk_bytes])
+        m_.crypto_sign_expandsk(esk, z.esk_bytes, 64, st)
         msgs = torch.from_numpy(tmsg[rows].copy()).to(dev)
         lens = torch.from_numpy(tmlen[rows].astype(np.int32)).to(dev)
         offs = torch.arange(64, dtype=torch.int64, device=dev) * max_msg
         sig = torch.zeros(64 * z.sig_bytes, dtype=torch.uint8, device=dev)
-        ws = torch.zeros(64 * M.Mayo(s).sign_ws_bytes(), dtype=torch.uint8, device=dev)
-        M.Mayo(s).sign_many(esk.reshape(-1), msgs.reshape(-1), sig, ws, 64, esk_stride=z.esk_bytes, msg_off=offs,
-                            msg_len=lens, stream=st)
+        ws = torch.zeros(64 * m_.sign_ws_bytes(), dtype=torch.uint8, device=dev)
+        m_.sign_many(esk, msgs.reshape(-1), sig, ws, 64, esk_stride=z.esk_bytes, msg_off=offs, msg_len=lens, stream=st)
         plain_bad += int((sig.cpu().numpy().reshape(64, z.sig_bytes) != tsig[rows, : z.sig_bytes]).any(1).sum())
 
     mismatches = [plain_bad]
+    sig_len = np.array([M.sizes(int(x)).sig_bytes if x in sets else 0 for x in range(6)], np.int64)
 
     def runner(arr, op, tidx, bad):
-        def fetch(lo, hi):
-            t = tidx[lo:hi].astype(np.uint64)
-            out = np.empty((hi - lo, SV.MAX_SIG), np.uint8)
-            sig_base = np.where(bad[lo:hi], np.uint64(tbad.ctypes.data), np.uint64(tsig.ctypes.data))
-            r = SV.make_requests(op[lo:hi], tset[t], tkey[t], tmlen[t], tmsg.ctypes.data + t * ROW_MSG,
-                                 sig_base + t * ROW_SIG, out.ctypes.data + np.arange(hi - lo, dtype=np.uint64) * ROW_SIG)
-            return r, out
-
-        def on_done(lo, hi, out):
-            t = tidx[lo:hi]
-            sg = op[lo:hi] == Q.OP_SIGN
-            nb = 0
-            for s_ in sets:
-                rows = np.flatnonzero(sg & (tset[t] == s_))
-                sb = M.sizes(s_).sig_bytes
-                nb += int((out[rows, :sb] != tsig[t[rows], :sb]).any(1).sum())
-            nb += int((out[: hi - lo][~sg, 0] != bad[lo:hi][~sg].astype(np.uint8)).sum())
-            mismatches[0] += nb
-
-        b0 = server.batches
-        lat, wall, bs = SV.run_open_loop(server, arr, fetch, on_done)
-        served_t = lat + arr
-        return lat, float(np.nanmax(served_t)), bs, server.batches - b0
+        """The open-loop run of the native server over these requests; every result checked."""
+        n = arr.size
+        t = tidx.astype(np.uint64)
+        sg = op == Q.OP_SIGN
+        out_len = np.where(sg, sig_len[tset[tidx]], 1)
+        out_off = np.zeros(n, np.int64)
+        out_off[1:] = np.cumsum(out_len[:-1])
+        out = np.zeros(int(out_len.sum()) + 1, np.uint8)
+        sig_base = np.where(bad, np.uint64(tbad.ctypes.data), np.uint64(tsig.ctypes.data))
+        r = SV.make_requests(op, tset[t], tkey[t], tmlen[t], tmsg.ctypes.data + t * ROW_MSG, sig_base + t * ROW_SIG,
+                             np.uint64(out.ctypes.data) + out_off.astype(np.uint64))
+        s0 = server.stats()
+        lat, _ = server.run_open_loop(r, arr)
+        s1 = server.stats()
+        nb = 0
+        for s_ in sets:
+            rows = np.flatnonzero(sg & (tset[tidx] == s_))
+            sb = int(sig_len[s_])
+            got = out[out_off[rows][:, None] + np.arange(sb)]
+            nb += int((got != tsig[tidx[rows], :sb]).any(1).sum())
+        nb += int((out[out_off[~sg]] != bad[~sg].astype(np.uint8)).sum())
+        nb += int(np.isnan(lat).sum())
+        mismatches[0] += nb
+        batches = s1["batches"] - s0["batches"]
+        admitted = s1["requests_admitted"] - s0["requests_admitted"]
+        return lat, float(np.nanmax(lat + arr)), (batches, admitted, s1["max_batch_seen"]), batches
 
     # closed-loop batched peak through the same path (every request waiting from t = 0)
     n_peak = max_batch * 12
@@ -1456,13 +1465,13 @@ def run_serving(args, dist: Dist):
     sweep, head = [], None
     clocks = Clocks(dist.local)
     clocks.start()
-    l0 = server.kernel_launches
+    l0 = server.stats()["kernel_launches"]
     for rate in rates:
         n = int(min(rate * 0.5, 1.2e6))
         arr, op, tidx, bad = serving_stream(seed, rate, n, n_tmpl, tmpl_base)
         lat, span, bs, nb = runner(arr, op, tidx, bad)
         row = dict(SV.latency_stats(lat), offered_per_s=rate, served_per_s=round(n / span, 1),
-                   batches=int(nb), mean_batch=round(float(bs.mean()), 1), max_batch=int(bs.max()))
+                   batches=int(nb), mean_batch=round(bs[1] / max(bs[0], 1), 1), max_batch=int(bs[2]))
         sweep.append(row)
         if rate == round(target, -3):
             head = row
@@ -1477,7 +1486,8 @@ def run_serving(args, dist: Dist):
         "config": {"workload": "serving: open-loop Poisson arrivals, 70 % verify / 30 % sign, sets 40/30/20/10, "
                                "4096 resident keys, continuous batching over the persistent queue",
                    "max_batch": max_batch, "inflight_batches": args.inflight, "msg_len": f"32..{max_msg} B",
-                   "key_cache_bytes": cache.nbytes(), "device_bytes": server.device_bytes, "budget_bytes": budget,
+                   "key_cache_bytes": key_cache_bytes, "device_bytes": server.device_bytes, "budget_bytes": budget,
+                   "loop": "native (mayo_b200_server_run_open_loop, C++)",
                    "value": "requests/s served at an offered load of 0.8 x the closed-loop batched peak"},
         "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"], "p999_ms": head["p999_ms"],
         "offered_per_s": head["offered_per_s"],
@@ -1489,7 +1499,7 @@ def run_serving(args, dist: Dist):
                 "note": "every number here is end to end (host request buffers in, host results out); "
                         "a step is one admitted batch"},
         "roofline": None,
-        "gpu_launches": server.kernel_launches - l0,
+        "gpu_launches": server.stats()["kernel_launches"] - l0,
         "clocks": clk,
         "result_mismatches": mismatches[0],
     }

@@ -536,22 +536,36 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
 // ---- sign ----
 // First attempt from the planes, in a CTA without engine staging (more CTAs per SM).  A singular
 // first attempt goes to the retry list; the fix-up kernel finishes it with the engine.
+// SH_TAIL_G instances per CTA (sign_attempt's interleaved elimination: the G pivot owners of a
+// step share one publish and the live columns fill whole warps); a CTA's last instances past the
+// batch repeat the batch's last instance and write nothing.
+#ifndef MAYO_TAIL_G
+#define MAYO_TAIL_G 2
+#endif
 template <int SET>
-__global__ void __launch_bounds__(SignCfg<SET>::NT, SET == 5 ? 5 : 1)  // MAYO_5: 5 CTAs per SM by registers
+struct TailShape {
+    static constexpr int G = MAYO_TAIL_G;  // instances per CTA
+    static constexpr int NT = SignCfg<SET>::NT * G;
+    static constexpr int MINB = SET == 5 ? 2 : 1;  // MAYO_5: held to a register budget
+};
+template <int SET>
+__global__ void __launch_bounds__(TailShape<SET>::NT, TailShape<SET>::MINB)
     sign_shared_tail_kernel(const uint8_t *esk, uint8_t *sig, size_t sig_stride, const uint8_t *wsi, size_t wsi_stride,
-                            const uint4 *planes, const uint4 *opl, uint32_t *ctl, uint32_t *retry) {
+                            const uint4 *planes, const uint4 *opl, uint32_t *ctl, uint32_t *retry, uint32_t batch) {
     using P = SharedProb<SET, false>;
-    extern __shared__ __align__(16) uint8_t smem[];
-    constexpr int NT = SignCfg<SET>::NT;
+    using C = SignCfg<SET, 0, true>;
+    constexpr int G = TailShape<SET>::G, NT = C::NT;
+    extern __shared__ __align__(16) uint8_t smem0[];
     if (ctl[0]) return;  // the product gave up: the fix-up kernel signs everything
-    const int tid = threadIdx.x;
-    const uint32_t inst = blockIdx.x;
-    sign_load_ws<SET, NT, true>(smem, tid, esk, wsi + (size_t)inst * wsi_stride);
-    if (sign_attempt<SET, NT, true>(smem, tid, esk, planes + (size_t)inst * P::PLANES)) {
-        sign_write<SET, NT, true>(smem, tid, esk, sig + (size_t)inst * sig_stride, opl);
-    } else if (tid == 0) {
-        retry[atomicAdd(&ctl[1], 1u)] = inst;
-    }
+    const int T = threadIdx.x, g = T / NT, tid = T % NT;
+    const uint32_t inst = blockIdx.x * G + (uint32_t)g;
+    const bool live = inst < batch;
+    const uint32_t src = live ? inst : batch - 1;
+    uint8_t *smem = smem0 + (size_t)g * C::total;
+    sign_load_ws<SET, NT, true>(smem, tid, esk, wsi + (size_t)src * wsi_stride);
+    const bool ok = sign_attempt<SET, NT, true, G>(smem0, T, esk, planes + (size_t)src * P::PLANES);
+    sign_write<SET, NT, true>(smem, tid, esk, ok && live ? sig + (size_t)inst * sig_stride : nullptr, opl);
+    if (!ok && live && tid == 0) retry[atomicAdd(&ctl[1], 1u)] = inst;
 }
 
 // Retries (attempts ctr >= 1 of the listed instances) with the engine, or every instance from
@@ -763,10 +777,11 @@ static int sign_shared_t(const SignIO &io0, uint8_t *ws, size_t batch, cudaStrea
     if (rc != ST_OK) return rc;
     uint32_t *ctl = reinterpret_cast<uint32_t *>(ws);
     uint32_t *retry = reinterpret_cast<uint32_t *>(ws + WSL::retry_off(batch));
-    if (!set_smem_attr(sign_shared_tail_kernel<SET>, CT::total)) return ST_CUDA;
-    sign_shared_tail_kernel<SET><<<(unsigned)batch, CT::NT, CT::total, st>>>(
+    constexpr int TG = TailShape<SET>::G;
+    if (!set_smem_attr(sign_shared_tail_kernel<SET>, TG * CT::total)) return ST_CUDA;
+    sign_shared_tail_kernel<SET><<<(unsigned)((batch + TG - 1) / TG), TailShape<SET>::NT, TG * CT::total, st>>>(
         io.esk, io.sig, io.sig_stride, io.ws, io.ws_stride, reinterpret_cast<const uint4 *>(ws + WSL::planes_off(batch)),
-        reinterpret_cast<const uint4 *>(ws + WSL::op_off()), ctl, retry);
+        reinterpret_cast<const uint4 *>(ws + WSL::op_off()), ctl, retry, (uint32_t)batch);
     tmark(st);
     if (!set_smem_attr(sign_shared_fix_kernel<SET>, CF::total)) return ST_CUDA;
     sign_shared_fix_kernel<SET><<<fix_grid(batch), CF::NT, CF::total, st>>>(

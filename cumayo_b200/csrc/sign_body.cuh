@@ -248,13 +248,28 @@ __device__ __forceinline__ void sign_next_vr(uint8_t *smem, int tid, int ctr) {
     __syncthreads();
 }
 
+template <int SET, int NT_, bool CP_, int G>
+__device__ __forceinline__ bool sign_eliminate(uint8_t *smem0, int T);
+
 // One attempt on the V || r in shared memory: x on success, x = r on a singular system.
-// Returns whether the system had full rank (uniform over the CTA).  All threads must call it.
+// Returns whether the system had full rank.  All threads of the CTA must call it.
 // `pre`, when given, holds this attempt's T_j[r] = P1[r] V_j (rows r < v) and M_j[b] = V_j L[:, b]
 // (rows v + b) as bit-plane groups [j][row][w], computed for a whole batch on the tensor cores
 // (op_shared.cu); the two engine passes over P1 and L are then skipped.
-template <int SET, int NT_, bool CP_ = false>
-__device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8_t *esk, const uint4 *pre = nullptr) {
+//
+// G instances per CTA (G * NT threads; instance g's shared memory at smem0 + g * C::total): thread
+// T works on instance T / NT as thread T % NT everywhere except in the elimination, where the
+// instances' columns are interleaved -- thread T owns column KO - T / G of instance T % G -- so
+// the G pivot owners of a step sit in one warp (one publish for G instances) and the live
+// columns of a step fill whole warps.  All control flow and barriers are the same for every
+// instance (nothing depends on the data), so the instances run one shared barrier sequence.
+// With G = 1 smem0 / T are the instance's shared memory / thread index.  `esk` and `pre` are the
+// thread's own instance's (T / NT).  The result is that instance's.
+template <int SET, int NT_, bool CP_ = false, int G = 1>
+__device__ __forceinline__ bool sign_attempt(uint8_t *smem0, int T, const uint8_t *esk, const uint4 *pre = nullptr) {
+    static_assert(G == 1 || G == 2 || G == 4, "instances per CTA");
+    const int tid = G == 1 ? T : T % SignCfg<SET, NT_, CP_>::NT;
+    uint8_t *smem = smem0 + (G == 1 ? 0 : (size_t)(T / SignCfg<SET, NT_, CP_>::NT) * SignCfg<SET, NT_, CP_>::total);
     MAYO_SIGN_VIEWS
     uint4 *masks = reinterpret_cast<uint4 *>(smem + C::off_masks);
     uint4 *bs = reinterpret_cast<uint4 *>(smem + C::off_bs);
@@ -475,6 +490,28 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
     }
     for (int i = tid; i < W * 4; i += NT) reinterpret_cast<uint32_t *>(rhsacc)[i] = 0;
     __syncthreads();
+    const bool ok_mine = sign_eliminate<SET, NT_, CP_, G>(smem0, T);
+    (void)ok_mine;
+    return reinterpret_cast<const int *>(smem + C::off_flag)[0] != 0;
+}
+
+// The elimination of sign_attempt (sample_solution, src/sign.cu:10-145) for the G instances of a
+// CTA: [A | y] (bit-plane columns in each instance's acol area), r from V || r; writes x and the
+// rank flag of every instance.  Returns the flag of the instance whose column this thread owns.
+template <int SET, int NT_, bool CP_, int G>
+__device__ __forceinline__ bool sign_eliminate(uint8_t *smem0, int T) {
+    using S = Set<SET>;
+    using C = SignCfg<SET, NT_, CP_>;
+    constexpr int W = C::W, NT = C::NT, KO = S::ko, CPT = C::CPT;
+    // interleaved columns: thread T takes column rank u = T / G of instance T % G
+    const int tid = G == 1 ? T : T / G;
+    uint8_t *smem = smem0 + (G == 1 ? 0 : (size_t)(T % G) * C::total);
+    uint4 *acol = reinterpret_cast<uint4 *>(smem + C::off_bs);    // [NCOL][W]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);  // [2][W + 3]
+    uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);  // [W]
+    const uint8_t *s_vr = smem + C::off_vr;
+    uint8_t *s_x = smem + C::off_xs;
+    int *s_flag = reinterpret_cast<int *>(smem + C::off_flag);
 
     // ---- Gauss-Jordan without data branches.  Thread owns columns c = KO - (tid + NT q): the RHS on
     // thread 0 and the columns still to update (c > pc) on the lowest threads, so the work of a
@@ -565,10 +602,11 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
     for (int q = 0; q < CPT; q++)
         if (KO - (tid + NT * q) == 0) publish(q, 0);
     __syncthreads();
-    // Warp w owns columns <= KO - 32 w, so after step KO - 32 w - 1 it has nothing left to update
-    // or publish: it leaves the loop, and the steps' barrier counts only the warps still in it
-    // (the lowest ones; a public function of the step).
-    const int last_step = KO - 32 * (tid >> 5) - 1;
+    // Warp w owns column ranks >= 32 w / G, i.e. columns <= KO - 32 w / G, so after step
+    // KO - 32 w / G - 1 it has nothing left to update or publish: it leaves the loop, and the
+    // steps' barrier counts only the warps still in it (the lowest ones; a public function of the
+    // step).
+    const int last_step = KO - 32 * (T >> 5) / G - 1;
 #pragma unroll 1
     for (int pc = 0; pc <= last_step; pc++) {
         // Every column right of pc: col ^= col[p] * F'  (eliminates row p elsewhere, normalises
@@ -605,8 +643,8 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
             for (int w = 0; w < W; w++) g4_madd(col[q][w], D[w], fm);
             if (c == pc + 1 && c < KO) publish(q, c);
         }
-        const int nw = (KO - 1 - pc) / 32 + 1;  // warps with a column > pc (or column pc + 1)
-        bar_sync(1, 32 * (nw < NT / 32 ? nw : NT / 32));
+        const int nw = G * (KO - 1 - pc) / 32 + 1;  // warps with a column > pc (or column pc + 1)
+        bar_sync(1, 32 * (nw < G * NT / 32 ? nw : G * NT / 32));
     }
     // rank test (sign.cu:107-115 rejects when the last echelon row is zero, i.e. rank < m): thread
     // 0 took part in every step, so its record of the pivot rows is complete
@@ -623,7 +661,7 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem, int tid, const uint8
 #pragma unroll
             for (int w = 0; w < W; w++) g4_st(rhsacc + w, col[q][w]);  // not a buffer still being read
     __syncthreads();
-    const bool ok = s_flag[0] != 0;
+    const bool ok = s_flag[0] != 0;  // this column's instance
 #pragma unroll
     for (int q = 0; q < CPT; q++) {
         const int c = KO - (tid + NT * q);
@@ -743,10 +781,12 @@ __device__ __forceinline__ void sign_write(uint8_t *smem, int tid, const uint8_t
         }
     }
     __syncthreads();
-    uint8_t *sigp = sig;
-    for (int bidx = tid; bidx < S::k * S::n / 2; bidx += NT)
-        sigp[bidx] = (uint8_t)(snib[2 * bidx] | (snib[2 * bidx + 1] << 4));
-    for (int i = tid; i < S::sk; i += NT) sigp[S::k * S::n / 2 + i] = s_key[S::digest + i];
+    uint8_t *sigp = sig;  // nullptr: compute only (an instance of a multi-instance CTA that writes nothing)
+    if (sigp) {
+        for (int bidx = tid; bidx < S::k * S::n / 2; bidx += NT)
+            sigp[bidx] = (uint8_t)(snib[2 * bidx] | (snib[2 * bidx + 1] << 4));
+        for (int i = tid; i < S::sk; i += NT) sigp[S::k * S::n / 2 + i] = s_key[S::digest + i];
+    }
 }
 
 }  // namespace mayo

@@ -1,20 +1,19 @@
-"""Serving loop for MAYO sign / verify requests on one GPU: continuous batching over the
-persistent work queue, with the expanded keys resident in HBM under a byte budget.
+"""Serving loop for MAYO sign / verify requests on one GPU: a thin mirror of the native server
+(mayo_b200_server_* in libmayo_b200.so, C++: cumayo_b200/csrc/serve_loop.cu).
 
-Requests arrive one by one (an open-loop Poisson stream in the benchmark).  The server keeps up
-to `inflight` batches on the GPU, each on its own stream with its own queue memory and staging
-buffers.  Whenever a batch slot is free and requests are waiting, the waiting requests (up to
-`max_batch`, oldest first) are admitted as one batch: their inputs are packed into one pinned
-host buffer and copied to the device in one transfer, the queue partitions the batch by
-(set, op) on the device and drains it with the per-(set, op) persistent kernels, and one
-transfer brings the signatures and verify results back.  A request's latency is the time from
-its arrival to the host seeing its batch's results.
+Requests (40-byte records pointing into the caller's host memory) join a waiting line.  The
+server keeps up to `inflight` batches on the GPU, each on its own stream with its own queue
+memory and staging buffers.  Whenever a batch slot is free and requests wait, the longest prefix
+of the line (up to `max_batch`) whose keys fit in the key tables is admitted as one batch: keys
+not resident are expanded into free table rows, the inputs are packed into one pinned buffer and
+copied to the device in one transfer, the work queue partitions the batch by (set, op) on the
+device and drains it with the per-(set, op) persistent kernels, and one transfer brings the
+signatures and verify results back.  A request's latency is the time from its arrival to the
+server unpacking its result.
 
 Keys are registered per parameter set by id (their seeds) and expanded (esk for signing, epk for
-verifying) on first use into a per-set table in HBM.  A full table evicts its least recently used
-keys that no in-flight batch references.  Admission is bounded by the tables too: a batch takes
-the longest prefix of the waiting requests whose keys fit beside the keys in-flight batches hold
-(launch() itself raises CacheFull for a batch that does not fit).
+verifying) on first use into a per-set table in HBM; a full table evicts its least recently used
+rows that no batch in flight uses.
 
 This module has no counterpart in the reference, which offers only the synchronous batched pool
 API (include/api.cuh).
@@ -22,162 +21,111 @@ API (include/api.cuh).
 from __future__ import annotations
 
 import ctypes
-import time
 
 import numpy as np
 
-from . import queue as Q
-from .api import A128, Mayo, MayoError, _check, lib, sizes
+from .api import MayoError, _check, lib, sizes
 
 SETS = (1, 2, 3, 5)
 MAX_SIG = max(sizes(s).sig_bytes for s in SETS)
+ERR_FULL = 5  # MAYO_B200_ERR_FULL
 
 
 class CacheFull(MayoError):
     pass
 
 
-def _align(x: int, a: int = 16) -> int:
-    return (x + a - 1) // a * a
+def capacity_for_budget(budget_bytes: int, n_keys: dict) -> dict:
+    """Key-table rows per set: all keys if they fit, else the budget split by each set's key bytes."""
+    need = {s: n * (sizes(s).esk_bytes + sizes(s).epk_bytes) for s, n in n_keys.items()}
+    total = sum(need.values())
+    if total <= budget_bytes:
+        return dict(n_keys)
+    return {s: max(1, int(n_keys[s] * budget_bytes / total)) for s in n_keys}
 
 
 # ---------------------------------------------------------------------------------------------
-# key table bookkeeping (host only)
+# key table (host only; native: mayo_b200_key_table_*)
 # ---------------------------------------------------------------------------------------------
+class _KeyTableStats(ctypes.Structure):
+    _fields_ = [("capacity", ctypes.c_uint32), ("n_keys", ctypes.c_uint32), ("pinned_slots", ctypes.c_uint32),
+                ("resident_keys", ctypes.c_uint32), ("misses", ctypes.c_uint64), ("evictions", ctypes.c_uint64)]
+
+
 class SlotTable:
-    """Key id -> slot map of one parameter set's key table, least-recently-used eviction.
-
-    `acquire` maps a batch's key ids to slots, choosing slots for the keys that are not resident
-    (empty slots first, then the least recently used unpinned ones, never one this batch uses)
-    and pins every slot the batch uses until `release`."""
+    """Key id -> row map of one parameter set's key table with least-recently-used eviction (the
+    native table the server uses).  `acquire` maps a batch's key ids to rows, choosing rows for
+    the keys that are not resident (empty rows first, then the least recently used unpinned
+    ones, never one this batch uses) and pins every row the batch uses until `release`."""
 
     def __init__(self, capacity: int, n_keys: int):
-        if capacity <= 0:
-            raise MayoError("key table needs at least one slot")
-        self.capacity = capacity
-        self.slot_of = np.full(n_keys, -1, np.int64)
-        self.key_of = np.full(capacity, -1, np.int64)
-        self.last = np.zeros(capacity, np.int64)
-        self.pins = np.zeros(capacity, np.int64)
-        self.tick = 0
-        self.misses = 0
-        self.evictions = 0
+        L = _bind()
+        self._h = L.mayo_b200_key_table_create(capacity, n_keys) if capacity > 0 and n_keys > 0 else None
+        if not self._h:
+            raise MayoError("key table needs at least one row and one key")
+        self.capacity, self.n_keys = capacity, n_keys
 
-    def acquire(self, key_ids: np.ndarray):
-        """Returns (slot per key id, missing key ids, their new slots, slots to release).  The
-        release handle may repeat slots: `pins[idx] += 1` with repeated indices adds once per
-        distinct slot, which is the one pin per batch wanted."""
-        key_ids = np.asarray(key_ids, np.int64)
-        if key_ids.size and (key_ids.min() < 0 or key_ids.max() >= self.slot_of.size):
-            raise MayoError("unknown key id")
-        self.tick += 1
-        slots = self.slot_of[key_ids]
-        miss = np.zeros(0, np.int64)
-        new_slots = np.zeros(0, np.int64)
-        if (slots < 0).any():
-            miss = np.unique(key_ids[slots < 0])
-            cand_mask = self.pins == 0
-            cand_mask[slots[slots >= 0]] = False
-            cand = np.flatnonzero(cand_mask)
-            if cand.size < miss.size:
-                raise CacheFull(f"{miss.size} keys to load, {cand.size} slots free of in-flight batches")
-            pri = np.where(self.key_of[cand] < 0, -1, self.last[cand])
-            pick = cand if cand.size == miss.size else cand[np.argpartition(pri, miss.size - 1)[:miss.size]]
-            old = self.key_of[pick]
-            self.evictions += int((old >= 0).sum())
-            self.slot_of[old[old >= 0]] = -1
-            self.key_of[pick] = miss
-            self.slot_of[miss] = pick
-            self.misses += int(miss.size)
-            new_slots = pick
-            slots = self.slot_of[key_ids]
-        self.last[slots] = self.tick
-        self.pins[slots] += 1
-        return slots, miss, new_slots, slots
-
-    def release(self, su: np.ndarray) -> None:
-        self.pins[su] -= 1
-
-    def can_load(self, key_ids: np.ndarray) -> bool:
-        """Whether acquire(key_ids) would find slots for its missing keys (no state change)."""
-        key_ids = np.asarray(key_ids, np.int64)
-        slots = self.slot_of[key_ids]
-        if (slots >= 0).all():
-            return True
-        nmiss = int(np.unique(key_ids[slots < 0]).size)
-        used = np.unique(slots[slots >= 0])
-        free = int((self.pins == 0).sum()) - int((self.pins[used] == 0).sum())
-        return free >= nmiss
-
-
-class KeyCache:
-    """Expanded keys resident in HBM: per parameter set, a table of `capacity[set]` esk rows and
-    as many epk rows, filled on first use from the registered seeds.  Expansion runs on the
-    stream of the batch that needs the keys; every later batch waits for it."""
-
-    def __init__(self, seeds: dict, capacity: dict, device=None):
-        import torch
-        self.dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
-        self.seeds = {s: np.ascontiguousarray(v, np.uint8) for s, v in seeds.items()}
-        self.tables, self.esk, self.epk, self.mayo = {}, {}, {}, {}
-        for s, sd in self.seeds.items():
-            z = sizes(s)
-            cap = int(min(capacity[s], len(sd)))
-            self.tables[s] = SlotTable(cap, len(sd))
-            self.esk[s] = torch.zeros(cap * z.esk_bytes, dtype=torch.uint8, device=self.dev)
-            self.epk[s] = torch.zeros(cap * z.epk_bytes, dtype=torch.uint8, device=self.dev)
-            self.mayo[s] = Mayo(s)
-        self.ready = None  # event after the last expansion
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _bind().mayo_b200_key_table_destroy(self._h)
+            self._h = None
 
     @staticmethod
-    def capacity_for_budget(budget_bytes: int, n_keys: dict) -> dict:
-        """Slots per set: all keys if they fit, else the budget split by each set's key bytes."""
-        need = {s: n * (sizes(s).esk_bytes + sizes(s).epk_bytes) for s, n in n_keys.items()}
-        total = sum(need.values())
-        if total <= budget_bytes:
-            return dict(n_keys)
-        return {s: max(1, int(n_keys[s] * budget_bytes / total)) for s in n_keys}
+    def _ids(key_ids) -> np.ndarray:
+        k = np.asarray(key_ids, np.int64)
+        if k.size and (k.min() < 0 or k.max() >= 1 << 32):
+            raise MayoError("unknown key id")
+        return np.ascontiguousarray(k.astype(np.uint32))
 
-    def nbytes(self) -> int:
-        return sum(int(t.numel()) for t in self.esk.values()) + sum(int(t.numel()) for t in self.epk.values())
+    def acquire(self, key_ids):
+        """Returns (row per key id, missing key ids, their new rows, rows to release)."""
+        ids = self._ids(key_ids)
+        n = ids.size
+        slots = np.zeros(n, np.int32)
+        miss = np.zeros(max(n, 1), np.uint32)
+        new = np.zeros(max(n, 1), np.int32)
+        nm = ctypes.c_uint32(0)
+        rc = _bind().mayo_b200_key_table_acquire(self._h, ids.ctypes.data, n, slots.ctypes.data, miss.ctypes.data,
+                                                 new.ctypes.data, ctypes.byref(nm))
+        if rc == ERR_FULL:
+            raise CacheFull("not enough key-table rows free of batches in flight")
+        _check(rc, "key_table_acquire")
+        k = nm.value
+        return slots.astype(np.int64), miss[:k].astype(np.int64), new[:k].astype(np.int64), slots
 
-    def acquire(self, set_id: int, key_ids: np.ndarray, stream):
-        slots, miss, new_slots, su = self.tables[set_id].acquire(key_ids)
-        if miss.size:
-            self._expand(set_id, miss, new_slots, stream)
-        return slots, su
+    def release(self, su) -> None:
+        su = np.ascontiguousarray(su, np.int32)
+        _check(_bind().mayo_b200_key_table_release(self._h, su.ctypes.data, su.size), "key_table_release")
 
-    def release(self, set_id: int, su: np.ndarray) -> None:
-        self.tables[set_id].release(su)
+    def can_load(self, key_ids) -> bool:
+        ids = self._ids(key_ids)
+        r = _bind().mayo_b200_key_table_can_load(self._h, ids.ctypes.data, ids.size)
+        if r < 0:
+            raise MayoError("unknown key id")
+        return r == 1
 
-    def wait(self, stream) -> None:
-        if self.ready is not None:
-            stream.wait_event(self.ready)
+    def _info(self) -> _KeyTableStats:
+        st = _KeyTableStats()
+        _check(_bind().mayo_b200_key_table_info(self._h, ctypes.byref(st)), "key_table_info")
+        return st
 
-    def _expand(self, s: int, key_ids: np.ndarray, slots: np.ndarray, stream) -> None:
-        """seed -> (pk via keypair_from_seed) -> esk, epk, written into the given slots."""
-        import torch
-        m, z = self.mayo[s], sizes(s)
-        n = int(key_ids.size)
-        with torch.cuda.stream(stream):
-            seeds = torch.from_numpy(self.seeds[s][key_ids]).to(self.dev, non_blocking=False)
-            kp, kpitch = m.alloc_pool("keypair", n, device=self.dev)
-            kp.view(n, kpitch)[:, : z.sk_bytes].copy_(seeds)
-            m.crypto_sign_keypair_from_seed(kp, kpitch, n, stream)
-            esk = torch.zeros(n * z.esk_bytes, dtype=torch.uint8, device=self.dev)
-            esk.view(n, z.esk_bytes)[:, : z.sk_bytes].copy_(seeds)
-            m.crypto_sign_expandsk(esk, z.esk_bytes, n, stream)
-            epk = torch.zeros(n * z.epk_bytes, dtype=torch.uint8, device=self.dev)
-            pk_off = A128(z.sk_bytes)
-            epk.view(n, z.epk_bytes)[:, z.p_bytes - 16: z.p_bytes - 16 + z.pk_bytes].copy_(
-                kp.view(n, kpitch)[:, pk_off: pk_off + z.pk_bytes])
-            m.crypto_sign_expandpk(epk, z.epk_bytes, n, stream)
-            idx = torch.from_numpy(slots).to(self.dev)
-            self.esk[s].view(-1, z.esk_bytes).index_copy_(0, idx, esk.view(n, z.esk_bytes))
-            self.epk[s].view(-1, z.epk_bytes).index_copy_(0, idx, epk.view(n, z.epk_bytes))
-            ev = torch.cuda.Event()
-            ev.record(stream)
-        self.ready = ev
+    @property
+    def evictions(self) -> int:
+        return int(self._info().evictions)
+
+    @property
+    def misses(self) -> int:
+        return int(self._info().misses)
+
+    @property
+    def slot_of(self) -> np.ndarray:
+        L = _bind()
+        return np.array([L.mayo_b200_key_table_slot_of(self._h, i) for i in range(self.n_keys)], np.int64)
+
+    @property
+    def pins(self) -> np.ndarray:
+        L = _bind()
+        return np.array([L.mayo_b200_key_table_pins(self._h, i) for i in range(self.capacity)], np.int64)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -213,8 +161,59 @@ def _bind():
                                            ctypes.c_size_t, ctypes.c_size_t, ctypes.POINTER(Layout)]
         L.mayo_b200_serve_unpack.restype = ctypes.c_int
         L.mayo_b200_serve_unpack.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(Layout), ctypes.c_void_p]
+        vp, u32, u64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64
+        L.mayo_b200_key_table_create.restype = vp
+        L.mayo_b200_key_table_create.argtypes = [u32, u32]
+        L.mayo_b200_key_table_destroy.restype = None
+        L.mayo_b200_key_table_destroy.argtypes = [vp]
+        L.mayo_b200_key_table_acquire.restype = ctypes.c_int
+        L.mayo_b200_key_table_acquire.argtypes = [vp, vp, u32, vp, vp, vp, ctypes.POINTER(u32)]
+        L.mayo_b200_key_table_release.restype = ctypes.c_int
+        L.mayo_b200_key_table_release.argtypes = [vp, vp, u32]
+        L.mayo_b200_key_table_can_load.restype = ctypes.c_int
+        L.mayo_b200_key_table_can_load.argtypes = [vp, vp, u32]
+        L.mayo_b200_key_table_info.restype = ctypes.c_int
+        L.mayo_b200_key_table_info.argtypes = [vp, ctypes.POINTER(_KeyTableStats)]
+        L.mayo_b200_key_table_slot_of.restype = ctypes.c_int32
+        L.mayo_b200_key_table_slot_of.argtypes = [vp, u32]
+        L.mayo_b200_key_table_pins.restype = ctypes.c_int32
+        L.mayo_b200_key_table_pins.argtypes = [vp, u32]
+        for f in ("device_bytes", "host_bytes"):
+            getattr(L, "mayo_b200_server_" + f).restype = ctypes.c_size_t
+            getattr(L, "mayo_b200_server_" + f).argtypes = [ctypes.POINTER(_ServerConfig)]
+        L.mayo_b200_server_create.restype = ctypes.c_int
+        L.mayo_b200_server_create.argtypes = [ctypes.POINTER(_ServerConfig), ctypes.POINTER(vp), vp, ctypes.c_size_t,
+                                              vp, ctypes.c_size_t, ctypes.POINTER(vp)]
+        L.mayo_b200_server_destroy.restype = ctypes.c_int
+        L.mayo_b200_server_destroy.argtypes = [vp]
+        L.mayo_b200_server_submit.restype = ctypes.c_int
+        L.mayo_b200_server_submit.argtypes = [vp, vp, u32, u64]
+        L.mayo_b200_server_progress.restype = ctypes.c_int
+        L.mayo_b200_server_progress.argtypes = [vp, vp, u32, ctypes.POINTER(u32)]
+        L.mayo_b200_server_drain.restype = ctypes.c_int
+        L.mayo_b200_server_drain.argtypes = [vp]
+        L.mayo_b200_server_get_stats.restype = ctypes.c_int
+        L.mayo_b200_server_get_stats.argtypes = [vp, ctypes.POINTER(_ServerStats)]
+        L.mayo_b200_server_preload.restype = ctypes.c_int
+        L.mayo_b200_server_preload.argtypes = [vp, ctypes.c_int, vp, u32]
+        L.mayo_b200_server_queue_error.restype = ctypes.c_int
+        L.mayo_b200_server_queue_error.argtypes = [vp]
+        L.mayo_b200_server_run_open_loop.restype = ctypes.c_int
+        L.mayo_b200_server_run_open_loop.argtypes = [vp, vp, vp, u32, ctypes.c_double, vp, ctypes.POINTER(ctypes.c_double)]
         L._serve_bound = True
     return L
+
+
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [("max_batch", ctypes.c_uint32), ("inflight", ctypes.c_uint32), ("max_msg", ctypes.c_uint32),
+                ("expand_chunk", ctypes.c_uint32), ("n_keys", ctypes.c_uint32 * 4), ("key_slots", ctypes.c_uint32 * 4)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_uint64) for f in ("batches", "requests_admitted", "requests_done", "max_batch_seen",
+                                               "kernel_launches", "keys_expanded", "key_misses", "key_evictions",
+                                               "waiting")] + [("batches_in_flight", ctypes.c_uint32),
+                                                              ("pad", ctypes.c_uint32)]
 
 
 def make_requests(op, set_id, key_id, mlen, msg_ptr, sig_ptr, out_ptr) -> np.ndarray:
@@ -280,190 +279,118 @@ def latency_stats(lat: np.ndarray) -> dict:
 
 
 # ---------------------------------------------------------------------------------------------
-# the server
+# the server (native: mayo_b200_server_*)
 # ---------------------------------------------------------------------------------------------
-class _Slot:
-    def __init__(self, server, idx):
-        import torch
-        self.idx = idx
-        self.stream = torch.cuda.Stream(device=server.dev)
-        self.queue = Q.Queue(capacity=server.max_batch + server.max_batch // 8 + 64, device=server.dev)
-        self.h_in = torch.empty(server.in_bytes, dtype=torch.uint8).pin_memory()
-        self.h_out = torch.empty(server.out_bytes, dtype=torch.uint8).pin_memory()
-        self.d_in = torch.empty(server.in_bytes, dtype=torch.uint8, device=server.dev)
-        self.d_out = torch.empty(server.out_bytes, dtype=torch.uint8, device=server.dev)
-        self.in_np = self.h_in.numpy()
-        self.out_np = self.h_out.numpy()
-        self.event = torch.cuda.Event()
-        self.busy = False
-        self.tag = self.keep = self.reqs = self.layout = None
-        self.pins = []
-
-
 class Server:
-    """Continuous-batching MAYO sign / verify server on one GPU.
+    """Continuous-batching MAYO sign / verify server on one GPU (the native server).
 
-    max_batch requests per batch, `inflight` batches on the GPU at once, messages up to
-    max_msg bytes.  Device memory: the key cache plus, per in-flight batch, the queue memory and
-    the staging buffers; `budget_bytes` bounds the total (MayoError if it does not fit)."""
+    seeds: {set: (n_keys, sk_bytes) uint8 array} -- key id = row; key_slots: {set: resident rows}
+    (default: every key).  max_batch requests per batch, `inflight` batches on the GPU at once,
+    messages up to max_msg bytes.  The device and pinned host memory the server needs are
+    allocated here (torch) and handed to it; `budget_bytes` bounds the device bytes."""
 
-    def __init__(self, cache: KeyCache, max_batch: int = 4096, inflight: int = 2, max_msg: int = 256,
-                 budget_bytes: int = 60 << 30):
-        self.cache = cache
-        self.dev = cache.dev
-        self.max_batch = max_batch
-        self.max_msg = max_msg
-        self.in_bytes = in_bytes(max_batch, max_msg)
-        self.out_bytes = out_bytes(max_batch)
-        self.slots = [_Slot(self, i) for i in range(inflight)]
-        self.device_bytes = cache.nbytes() + sum(int(s.queue.mem.numel()) + int(s.queue.items.numel()) * 4 +
-                                                 self.in_bytes + self.out_bytes for s in self.slots)
-        if self.device_bytes > budget_bytes:
-            raise MayoError(f"server needs {self.device_bytes} device bytes, budget {budget_bytes}")
-        self.batches = 0
-        self.kernel_launches = 0
-
-    def free_slot(self):
-        for s in self.slots:
-            if not s.busy:
-                return s
-        return None
-
-    def fits(self, reqs: np.ndarray, k: int) -> bool:
-        """Whether the first k requests' keys can all be made resident now."""
-        for s in SETS:
-            rows = reqs["set"][:k] == s
-            if rows.any() and not self.cache.tables[s].can_load(reqs["key_id"][:k][rows]):
-                return False
-        return True
-
-    def admit_len(self, reqs: np.ndarray) -> int:
-        """The longest prefix of reqs (at most max_batch) whose keys fit in the key tables beside
-        the keys in-flight batches hold; 0 = wait for a batch to finish."""
-        k = min(int(reqs.size), self.max_batch)
-        if self.fits(reqs, k):
-            return k
-        lo, hi = 0, k  # fits(lo) holds, fits(hi) does not
-        while hi - lo > 1:
-            mid = (lo + hi) // 2
-            if self.fits(reqs, mid):
-                lo = mid
-            else:
-                hi = mid
-        return lo
-
-    def launch(self, reqs: np.ndarray, tag=None, keep=None) -> _Slot:
-        """Admit one batch of request records (REQ_DTYPE; asynchronous).  The records and the
-        memory they point to (`keep` holds whatever must stay alive) belong to the server until
-        poll() returns the batch.  Raises if no slot is free or the keys do not fit."""
+    def __init__(self, seeds: dict, key_slots: dict | None = None, max_batch: int = 4096, inflight: int = 2,
+                 max_msg: int = 256, budget_bytes: int = 60 << 30, device=None, expand_chunk: int = 0):
         import torch
-        slot = self.free_slot()
-        if slot is None:
-            raise MayoError("no free batch slot")
-        n = int(reqs.size)
-        if n == 0 or n > self.max_batch:
-            raise MayoError(f"batch of {n} requests (max {self.max_batch})")
-        st = slot.stream
-        pins = []
+        L = _bind()
+        self.dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.max_batch, self.max_msg = max_batch, max_msg
+        cfg = _ServerConfig(max_batch, inflight, max_msg, expand_chunk)
+        self._seeds = []
+        ptrs = (ctypes.c_void_p * 4)()
+        for i, s in enumerate(SETS):
+            if s in seeds:
+                a = np.ascontiguousarray(seeds[s], np.uint8)
+                if a.ndim != 2 or a.shape[1] != sizes(s).sk_bytes:
+                    raise MayoError(f"MAYO_{s} seeds must be (n, {sizes(s).sk_bytes}) uint8")
+                self._seeds.append(a)
+                cfg.n_keys[i] = a.shape[0]
+                cfg.key_slots[i] = int((key_slots or {}).get(s, 0))
+                ptrs[i] = a.ctypes.data
+        with torch.cuda.device(self.dev):
+            dbytes = L.mayo_b200_server_device_bytes(ctypes.byref(cfg))
+            hbytes = L.mayo_b200_server_host_bytes(ctypes.byref(cfg))
+        if dbytes == 0 or hbytes == 0:
+            raise MayoError("invalid server configuration")
+        if dbytes > budget_bytes:
+            raise MayoError(f"server needs {dbytes} device bytes, budget {budget_bytes}")
+        self.device_bytes, self.host_bytes = int(dbytes), int(hbytes)
+        self._dmem = torch.empty(dbytes + 256, dtype=torch.uint8, device=self.dev)
+        self._hmem = torch.empty(hbytes + 256, dtype=torch.uint8).pin_memory()
+        dp = (self._dmem.data_ptr() + 255) // 256 * 256
+        hp = (self._hmem.data_ptr() + 255) // 256 * 256
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.dev):
+            _check(L.mayo_b200_server_create(ctypes.byref(cfg), ptrs, dp, dbytes, hp, hbytes, ctypes.byref(h)),
+                   "server_create")
+        self._h = h
+        self._keep = {}  # tag -> objects whose memory requests point into, until done
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _check(_bind().mayo_b200_server_destroy(self._h), "server_destroy")
+            self._h = None
+
+    def __del__(self):
         try:
-            for s in SETS:
-                rows = np.flatnonzero(reqs["set"] == s)
-                if rows.size:
-                    ks, su = self.cache.acquire(s, reqs["key_id"][rows], st)
-                    pins.append((s, su))
-                    reqs["key_slot"][rows] = ks
-            lay = pack(reqs, self.max_msg, slot.in_np, slot.out_np.size)
+            self.close()
         except Exception:
-            for s, su in pins:
-                self.cache.release(s, su)
-            raise
-        q = slot.queue
-        base_in, base_out = slot.d_in.data_ptr(), slot.d_out.data_ptr()
-        ops = {s: Q.SetOperands(kp_count=0, sg_count=0, vf_count=0) for s in SETS}
-        groups = 0
-        for g in lay.group:
-            if not g.count:
-                continue
-            groups += 1
-            o, tab = ops[g.set], self.cache.tables[g.set]
-            if g.op == Q.OP_SIGN:
-                o.sg_esk, o.sg_nkeys, o.sg_key = self.cache.esk[g.set], tab.capacity, base_in + g.key_off
-                o.sg_msg, o.sg_msg_len, o.sg_mlen = base_in + g.msg_off, base_in + g.len_off, self.max_msg
-                o.sg_sig, o.sg_count = base_out + g.out_off, g.count
-            else:
-                o.vf_epk, o.vf_nkeys, o.vf_key = self.cache.epk[g.set], tab.capacity, base_in + g.key_off
-                o.vf_msg, o.vf_msg_len, o.vf_mlen = base_in + g.msg_off, base_in + g.len_off, self.max_msg
-                o.vf_sig, o.vf_res, o.vf_count = base_in + g.sig_off, base_out + g.out_off, g.count
-        for s, o in ops.items():
-            q.set_operands(s, o)
-        with torch.cuda.stream(st):
-            self.cache.wait(st)
-            slot.d_in[: lay.in_bytes].copy_(slot.h_in[: lay.in_bytes], non_blocking=True)
-            q.run_items(base_in, n, stream=st)
-            slot.h_out[: lay.out_bytes].copy_(slot.d_out[: lay.out_bytes], non_blocking=True)
-            slot.event.record(st)
-        slot.busy, slot.tag, slot.keep, slot.reqs, slot.layout, slot.pins = True, tag, keep, reqs, lay, pins
-        self.batches += 1
-        self.kernel_launches += 2 + groups  # queue fill + partition + one persistent kernel per group
-        return slot
+            pass
 
-    def poll(self):
-        """Finished batches, their results unpacked into the requests' `out`: [(tag, keep)]."""
-        done = []
-        for slot in self.slots:
-            if slot.busy and slot.event.query():
-                unpack(slot.reqs, slot.layout, slot.out_np)
-                done.append((slot.tag, slot.keep))
-                for s, su in slot.pins:
-                    self.cache.release(s, su)
-                slot.busy, slot.pins, slot.reqs, slot.keep = False, [], None, None
-        return done
+    def preload(self, set_id: int, key_ids) -> None:
+        """Makes the keys resident now (only while no batch is in flight)."""
+        ids = np.ascontiguousarray(np.asarray(key_ids, np.int64).astype(np.uint32))
+        _check(_bind().mayo_b200_server_preload(self._h, set_id, ids.ctypes.data, ids.size), "server_preload")
 
-    def drain(self):
+    def submit(self, reqs: np.ndarray, first_tag: int = 0, keep=None) -> None:
+        """Requests join the waiting line; request i gets tag first_tag + i.  The memory the
+        records point into must stay alive until they are done (`keep` holds it until then)."""
+        reqs = np.ascontiguousarray(reqs, REQ_DTYPE)
+        _check(_bind().mayo_b200_server_submit(self._h, reqs.ctypes.data, reqs.size, first_tag), "server_submit")
+        if keep is not None:
+            self._keep[first_tag] = keep
+
+    def progress(self, cap: int = 1 << 16) -> np.ndarray:
+        """One non-blocking pass; returns the tags of requests finished since the last call."""
+        buf = np.zeros(cap, np.uint64)
+        n = ctypes.c_uint32(0)
+        _check(_bind().mayo_b200_server_progress(self._h, buf.ctypes.data, cap, ctypes.byref(n)), "server_progress")
+        return buf[: n.value]
+
+    def drain(self) -> np.ndarray:
+        """Serves everything submitted; returns the tags finished since the last progress()."""
+        rc = _bind().mayo_b200_server_drain(self._h)
+        if rc == ERR_FULL:
+            raise CacheFull("waiting requests need more key-table rows than exist")
+        _check(rc, "server_drain")
         out = []
-        while any(s.busy for s in self.slots):
-            out += self.poll()
-        return out
+        while True:
+            t = self.progress()
+            if t.size == 0:
+                break
+            out.append(t)
+        self._keep.clear()
+        return np.concatenate(out) if out else np.zeros(0, np.uint64)
+
+    def run_open_loop(self, reqs: np.ndarray, arrivals: np.ndarray, time_limit: float = 0.0):
+        """Open-loop run (native): request i arrives arrivals[i] seconds after the start.
+        Returns (latency per request in seconds, NaN if not served; wall seconds)."""
+        reqs = np.ascontiguousarray(reqs, REQ_DTYPE)
+        arr = np.ascontiguousarray(arrivals, np.float64)
+        lat = np.full(reqs.size, np.nan)
+        wall = ctypes.c_double(0.0)
+        _check(_bind().mayo_b200_server_run_open_loop(self._h, reqs.ctypes.data, arr.ctypes.data, reqs.size,
+                                                      float(time_limit), lat.ctypes.data, ctypes.byref(wall)),
+               "server_run_open_loop")
+        return lat, wall.value
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        _check(_bind().mayo_b200_server_get_stats(self._h, ctypes.byref(st)), "server_get_stats")
+        return {f: int(getattr(st, f)) for f, _ in _ServerStats._fields_ if f != "pad"}
 
     def check_queue(self) -> None:
-        """Raise if any slot's last run reported a queue error (synchronises)."""
-        for s in self.slots:
-            st = s.queue.stats()
-            if st["error"] != Q.QUEUE_OK:
-                raise MayoError(f"queue error {st['error']}")
-
-
-def run_open_loop(server: Server, arrivals: np.ndarray, fetch, on_done=None, time_limit: float = None):
-    """Serve requests arriving at `arrivals` (seconds from the start, sorted).  fetch(lo, hi)
-    returns (request records for rows lo..hi-1, an object keeping their memory alive);
-    on_done(lo, hi, keep) sees each finished batch.  Returns (latency per request in seconds,
-    NaN if not served; wall seconds; batch sizes)."""
-    n = int(arrivals.size)
-    done_t = np.full(n, np.nan)
-    nxt, finished = 0, 0
-    sizes_ = []
-    t0 = time.perf_counter()
-    while finished < n:
-        now = time.perf_counter() - t0
-        for (lo, hi), keep in server.poll():
-            done_t[lo:hi] = time.perf_counter() - t0
-            finished += hi - lo
-            if on_done is not None:
-                on_done(lo, hi, keep)
-        if nxt < n and server.free_slot() is not None:
-            ready = int(np.searchsorted(arrivals, now, side="right"))
-            if ready > nxt:
-                reqs, keep = fetch(nxt, min(ready, nxt + server.max_batch))
-                k = server.admit_len(reqs)  # bounded by the key tables
-                if k:
-                    server.launch(reqs[:k], tag=(nxt, nxt + k), keep=keep)
-                    sizes_.append(k)
-                    nxt += k
-        if time_limit is not None and now > time_limit:
-            for (lo, hi), keep in server.drain():
-                done_t[lo:hi] = time.perf_counter() - t0
-                if on_done is not None:
-                    on_done(lo, hi, keep)
-            break
-    wall = time.perf_counter() - t0
-    return done_t - arrivals, wall, np.array(sizes_, np.int64)
+        """Raise if any batch slot's last queue run reported an error (synchronises)."""
+        err = _bind().mayo_b200_server_queue_error(self._h)
+        if err != 0:
+            raise MayoError(f"queue error {err}")

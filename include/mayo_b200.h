@@ -40,6 +40,7 @@ typedef enum mayo_b200_status {
     MAYO_B200_ERR_ARG = 2,  /* null pointer, pitch too small, message too long, ... */
     MAYO_B200_ERR_CUDA = 3, /* a CUDA call failed; see mayo_b200_last_cuda_error() */
     MAYO_B200_ERR_TOO_LARGE = 4, /* batch exceeds mayo_b200_sign_noalloc_max_batch(set) */
+    MAYO_B200_ERR_FULL = 5, /* key table: not enough rows free of batches in flight */
 } mayo_b200_status;
 
 /* Byte sizes of one parameter set (reference include/params.h:10-92 and derived sizes). */
@@ -322,6 +323,93 @@ MAYO_B200_API int mayo_b200_serve_pack(const mayo_b200_serve_req *req, uint32_t 
                                        mayo_b200_serve_layout *layout);
 MAYO_B200_API int mayo_b200_serve_unpack(const mayo_b200_serve_req *req, uint32_t n,
                                          const mayo_b200_serve_layout *layout, const uint8_t *stage_out);
+
+/* ---- Extension (no counterpart in the reference): the serving loop (host code, C++) ----
+ * Continuous batching of sign / verify requests (mayo_b200_serve_req) over the work queue, with
+ * the expanded keys resident on the GPU.  Keys are registered per parameter set as their
+ * sk_bytes seeds (key id = row of the seed array; the caller keeps the seeds alive for the
+ * server's life) and expanded (keypair -> esk, epk) on first use into that set's key table of
+ * `key_slots` rows; a full table evicts its least recently used rows that no batch in flight
+ * uses.  Up to `inflight` batches are on the GPU at once, each with its own stream, queue memory
+ * and staging.  The caller provides all memory: mayo_b200_server_device_bytes of device memory
+ * and mayo_b200_server_host_bytes of pinned host memory (both 256-byte aligned); the server
+ * creates CUDA streams and events only.  One host thread at a time may call a server.
+ *
+ * Key table (host only, usable on its own): key id -> row, least-recently-used eviction,
+ * pinning.  acquire maps a batch's key ids to rows (slots[i] for key_ids[i]), loads the missing
+ * ids into unpinned rows the batch does not use (empty rows first, then the least recently used)
+ * and reports them (distinct ids and their rows), and pins every distinct row the batch uses
+ * once; MAYO_B200_ERR_FULL (and no change) when too few rows are free; MAYO_B200_ERR_ARG for an
+ * unknown id.  release unpins every distinct row among the given slots once (the slots one
+ * acquire returned).  can_load: 1 if acquire would succeed, 0 if not, -1 on bad arguments. */
+typedef struct mayo_b200_key_table mayo_b200_key_table;
+typedef struct mayo_b200_key_table_stats {
+    uint32_t capacity, n_keys, pinned_slots, resident_keys;
+    uint64_t misses, evictions;
+} mayo_b200_key_table_stats;
+MAYO_B200_API mayo_b200_key_table *mayo_b200_key_table_create(uint32_t capacity, uint32_t n_keys);
+MAYO_B200_API void mayo_b200_key_table_destroy(mayo_b200_key_table *t);
+MAYO_B200_API int mayo_b200_key_table_acquire(mayo_b200_key_table *t, const uint32_t *key_ids, uint32_t n,
+                                              int32_t *slots, uint32_t *miss_ids, int32_t *miss_slots,
+                                              uint32_t *n_miss);
+MAYO_B200_API int mayo_b200_key_table_release(mayo_b200_key_table *t, const int32_t *slots, uint32_t n);
+MAYO_B200_API int mayo_b200_key_table_can_load(mayo_b200_key_table *t, const uint32_t *key_ids, uint32_t n);
+MAYO_B200_API int mayo_b200_key_table_info(const mayo_b200_key_table *t, mayo_b200_key_table_stats *out);
+MAYO_B200_API int32_t mayo_b200_key_table_slot_of(const mayo_b200_key_table *t, uint32_t key_id); /* -1: not resident */
+MAYO_B200_API int32_t mayo_b200_key_table_pins(const mayo_b200_key_table *t, uint32_t slot);
+
+typedef struct mayo_b200_server mayo_b200_server;
+typedef struct mayo_b200_server_config {
+    uint32_t max_batch;    /* requests per batch (<= 2^20) */
+    uint32_t inflight;     /* batches on the GPU at once */
+    uint32_t max_msg;      /* longest message, bytes */
+    uint32_t expand_chunk; /* keys per expansion launch (scratch rows); 0 = 256 */
+    uint32_t n_keys[4];    /* registered keys of MAYO_1, 2, 3, 5 */
+    uint32_t key_slots[4]; /* resident rows per set (0 or >= n_keys: every key) */
+} mayo_b200_server_config;
+typedef struct mayo_b200_server_stats {
+    uint64_t batches, requests_admitted, requests_done, max_batch_seen, kernel_launches, keys_expanded;
+    uint64_t key_misses, key_evictions, waiting;
+    uint32_t batches_in_flight, pad;
+} mayo_b200_server_stats;
+/* Memory the caller provides for `cfg` on the current device (0 on a bad configuration). */
+MAYO_B200_API size_t mayo_b200_server_device_bytes(const mayo_b200_server_config *cfg);
+MAYO_B200_API size_t mayo_b200_server_host_bytes(const mayo_b200_server_config *cfg);
+/* seeds[i]: n_keys[i] * sk_bytes of set i (NULL where n_keys[i] is 0), host memory. */
+MAYO_B200_API int mayo_b200_server_create(const mayo_b200_server_config *cfg, const uint8_t *const seeds[4],
+                                          void *device_mem, size_t device_bytes, void *host_pinned,
+                                          size_t host_bytes, mayo_b200_server **out);
+/* Waits for the batches in flight, then frees the server (not the caller's memory). */
+MAYO_B200_API int mayo_b200_server_destroy(mayo_b200_server *srv);
+/* Appends n requests to the waiting line; request i gets tag first_tag + i.  The records are
+ * copied; the memory they point to (message, signature, out) must stay valid until the request
+ * is reported done.  Checks every request first (MAYO_B200_ERR_ARG: unknown set or key id, op
+ * other than sign / verify, mlen > max_msg, missing pointer) and takes none on error. */
+MAYO_B200_API int mayo_b200_server_submit(mayo_b200_server *srv, const mayo_b200_serve_req *req, uint32_t n,
+                                          uint64_t first_tag);
+/* One non-blocking pass: batches that finished are unpacked into their requests' `out` and their
+ * rows released; free batch slots admit the longest prefix of the waiting line (<= max_batch)
+ * whose keys fit; up to `cap` tags of finished requests go to done_tags (*n_done of them; the
+ * rest wait for the next call). */
+MAYO_B200_API int mayo_b200_server_progress(mayo_b200_server *srv, uint64_t *done_tags, uint32_t cap,
+                                            uint32_t *n_done);
+/* Runs progress until nothing waits and nothing is in flight (tags stay for progress to
+ * report); MAYO_B200_ERR_FULL if requests wait whose keys can never fit the tables. */
+MAYO_B200_API int mayo_b200_server_drain(mayo_b200_server *srv);
+MAYO_B200_API int mayo_b200_server_get_stats(const mayo_b200_server *srv, mayo_b200_server_stats *out);
+/* Makes keys resident ahead of their requests (expands the missing ones; waits until done).
+ * Only on an idle server (no batch in flight); MAYO_B200_ERR_ARG for an unknown set or key id. */
+MAYO_B200_API int mayo_b200_server_preload(mayo_b200_server *srv, int set, const uint32_t *key_ids, uint32_t n);
+/* First queue error code (MAYO_B200_QUEUE_*) in the slots' last runs; waits for them; -1 on a
+ * CUDA error. */
+MAYO_B200_API int mayo_b200_server_queue_error(mayo_b200_server *srv);
+/* Open-loop run on an idle server: request i joins the waiting line once arrival_s[i] seconds
+ * (sorted) have passed since the call began, and latency_s[i] = the time its result was unpacked
+ * minus arrival_s[i] (NaN if not served).  With time_limit_s > 0, no request is admitted after
+ * that time (the batches in flight finish).  *wall_s = the run's duration. */
+MAYO_B200_API int mayo_b200_server_run_open_loop(mayo_b200_server *srv, const mayo_b200_serve_req *req,
+                                                 const double *arrival_s, uint32_t n, double time_limit_s,
+                                                 double *latency_s, double *wall_s);
 
 /* ---- Sign without caller workspace.  No counterpart in the reference API. ----
  * For callers that cannot allocate device memory (a service whose device-memory budget is

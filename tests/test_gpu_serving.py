@@ -51,16 +51,12 @@ def _case(seed=9, n=240, keys_per_set=5):
     return seeds, _Case(op.astype(np.uint8), set_id.astype(np.uint8), key, mlen, msg, sig), want_sig, want_res
 
 
-class _Batch:
-    """Request records for rows lo..hi-1 of the case, with their output rows."""
-
-    def __init__(self, req, lo, hi):
-        sl = slice(lo, hi)
-        self.out = np.zeros((hi - lo, SV.MAX_SIG), np.uint8)
-        self.msg = np.ascontiguousarray(req.msg[sl])
-        self.sig = np.ascontiguousarray(req.sig[sl])
-        self.reqs = SV.requests_from_rows(req.op[sl], req.set_id[sl], req.key[sl], req.mlen[sl], self.msg, self.sig,
-                                          self.out)
+def _rows(req, lo, hi, out):
+    """Request records for rows lo..hi-1 of the case, results into `out` (rows 0..hi-lo-1)."""
+    sl = slice(lo, hi)
+    msg = np.ascontiguousarray(req.msg[sl])
+    sig = np.ascontiguousarray(req.sig[sl])
+    return SV.requests_from_rows(req.op[sl], req.set_id[sl], req.key[sl], req.mlen[sl], msg, sig, out), (msg, sig)
 
 
 def _check(req, lo, hi, out, want_sig, want_res):
@@ -73,30 +69,49 @@ def _check(req, lo, hi, out, want_sig, want_res):
 
 
 def test_serving_mix_and_alone_match_oracle(cuda):
+    """The native server's open-loop run: admission, batching, key eviction and reload while
+    batches are in flight; then single requests through submit / drain."""
     seeds, req, want_sig, want_res = _case()
-    cache = SV.KeyCache(seeds, {s: 3 for s in SETS})  # 3 slots for 5 keys per set
-    server = SV.Server(cache, max_batch=32, inflight=2, max_msg=MAX_MSG)
-    arrivals = SV.poisson_arrivals(4e3, len(req), b"serving-test".ljust(32, b"\0"))
-    done = []
-
-    def fetch(lo, hi):
-        b = _Batch(req, lo, hi)
-        return b.reqs, b
-
-    def on_done(lo, hi, b):  # the batch may be a prefix of what fetch returned
-        done.append((lo, hi, b))
-
-    lat, wall, sizes_ = SV.run_open_loop(server, arrivals, fetch, on_done)
-    assert np.isfinite(lat).all() and (lat >= 0).all()
+    n = len(req)
+    server = SV.Server(seeds, key_slots={s: 3 for s in SETS}, max_batch=32, inflight=2, max_msg=MAX_MSG)
+    arrivals = SV.poisson_arrivals(4e3, n, b"serving-test".ljust(32, b"\0"))
+    out = np.zeros((n, SV.MAX_SIG), np.uint8)
+    reqs, keep = _rows(req, 0, n, out)
+    lat, wall = server.run_open_loop(reqs, arrivals)
+    assert np.isfinite(lat).all() and (lat >= 0).all() and wall > 0
     server.check_queue()
-    assert sum(hi - lo for lo, hi, _ in done) == len(req)
-    for lo, hi, b in done:
-        _check(req, lo, hi, b.out, want_sig, want_res)
-    assert sum(t.evictions for t in cache.tables.values()) > 0  # the table really was too small
+    _check(req, 0, n, out, want_sig, want_res)
+    st = server.stats()
+    assert st["requests_done"] == n and st["batches"] > 1 and st["max_batch_seen"] <= 32
+    assert st["key_evictions"] > 0  # the tables really were too small
     # the same requests one per batch
-    for i in range(0, len(req), 7):
-        b = _Batch(req, i, i + 1)
-        server.launch(b.reqs, tag=(i, i + 1), keep=b)
-        server.drain()
-        _check(req, i, i + 1, b.out, want_sig, want_res)
+    for i in range(0, n, 7):
+        o1 = np.zeros((1, SV.MAX_SIG), np.uint8)
+        r1, k1 = _rows(req, i, i + 1, o1)
+        server.submit(r1, first_tag=i, keep=k1)
+        assert server.drain().tolist() == [i]
+        _check(req, i, i + 1, o1, want_sig, want_res)
+    # several batches through submit / progress, tags reported once each
+    out2 = np.zeros((n, SV.MAX_SIG), np.uint8)
+    r2, k2 = _rows(req, 0, n, out2)
+    server.submit(r2, first_tag=1000)
+    tags = []
+    while len(tags) < n:
+        tags += server.progress().tolist()
+    assert sorted(tags) == list(range(1000, 1000 + n))
+    _check(req, 0, n, out2, want_sig, want_res)
     server.check_queue()
+    server.close()
+
+
+def test_serving_rejects_bad_requests(cuda):
+    seeds, req, _, _ = _case(n=8)
+    server = SV.Server(seeds, max_batch=8, inflight=1, max_msg=MAX_MSG)
+    out = np.zeros((8, SV.MAX_SIG), np.uint8)
+    reqs, keep = _rows(req, 0, 8, out)
+    bad = reqs.copy()
+    bad["key_id"][3] = 99  # 5 keys per set
+    with pytest.raises(SV.MayoError):
+        server.submit(bad)
+    assert server.stats()["waiting"] == 0  # nothing taken
+    server.close()

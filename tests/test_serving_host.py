@@ -56,8 +56,8 @@ def test_slot_table_can_load_matches_acquire():
 
 def test_capacity_for_budget():
     n = {1: 10, 5: 4}
-    assert SV.KeyCache.capacity_for_budget(1 << 40, n) == n
-    cap = SV.KeyCache.capacity_for_budget(4 * (sizes(1).esk_bytes + sizes(1).epk_bytes), n)
+    assert SV.capacity_for_budget(1 << 40, n) == n
+    cap = SV.capacity_for_budget(4 * (sizes(1).esk_bytes + sizes(1).epk_bytes), n)
     assert 1 <= cap[1] < 10 and 1 <= cap[5] < 4
 
 
