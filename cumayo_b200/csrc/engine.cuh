@@ -20,6 +20,10 @@
 
 #include "common.cuh"
 
+#ifndef MAYO_ENGINE_X4
+#define MAYO_ENGINE_X4 0
+#endif
+
 namespace mayo {
 
 // Packed bytes [p, p + n) (n <= 16) of an m-vector group as four LE words, touching only
@@ -152,6 +156,9 @@ struct Engine {
     // T_j[r] for this thread's (j, w) over row r = r0 + rs (call only when active and r < nrows).
     template <class Rows>
     __device__ __forceinline__ G4 row_product(const Rows &rows, int r) const {
+#if MAYO_ENGINE_X4
+        return row_product_x4(rows, r);
+#else
         G4 acc = g4_zero();
         const int cnt = rows.count(r);
         const uint4 *bp = bs + (size_t)rs * MAXE * W + w;
@@ -164,6 +171,24 @@ struct Engine {
             g4_madd(acc, v, m);
         }
         return acc;
+#endif
+    }
+    // The same with four partial sums, one per power of x, folded once at the end of the row
+    // (g4x4_madd): three XORs fewer per entry, twelve more live registers.
+    template <class Rows>
+    __device__ __forceinline__ G4 row_product_x4(const Rows &rows, int r) const {
+        G4x4 acc = g4x4_zero();
+        const int cnt = rows.count(r);
+        const uint4 *bp = bs + (size_t)rs * MAXE * W + w;
+        const int c0 = rows.col(r, 0);
+        const uint4 *mp = masks + (size_t)c0 * J + j;
+#pragma unroll 4
+        for (int e = 0; e < cnt; e++) {
+            const G4 v = g4_ld(bp + e * W);
+            const uint4 m = mp[e * J];
+            g4x4_madd(acc, v, m);
+        }
+        return g4x4_fold(acc);
     }
 };
 

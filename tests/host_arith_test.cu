@@ -58,6 +58,19 @@ int main() {
         const uint32_t rw[4] = {r.x, r.y, r.z, r.w};
         for (int c = 0; c < 32; c++)
             if (nib(rw, c) != (nib(a0, c) ^ ref_mul(nib(w, c), s))) FAIL("g4_madd it=%d c=%d", it, c);
+        // the four-partial-sum form of a sum of products equals the g4_madd sum
+        {
+            G4 ref = g4_zero();
+            G4x4 A = g4x4_zero();
+            for (int q = 0; q < 5; q++) {
+                const G4 v = g4_from_packed(rnd(), rnd(), rnd(), rnd());
+                const uint4 mk = scalar_masks(rnd() & 0xF);
+                g4_madd(ref, v, mk);
+                g4x4_madd(A, v, mk);
+            }
+            const G4 f = g4x4_fold(A);
+            if (f.p0 != ref.p0 || f.p1 != ref.p1 || f.p2 != ref.p2 || f.p3 != ref.p3) FAIL("g4x4_madd it=%d", it);
+        }
         // eight packed nibbles times a public constant
         uint32_t m = nib8_mul_const(w[0], s);
         for (int c = 0; c < 8; c++)
