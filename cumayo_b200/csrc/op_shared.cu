@@ -540,7 +540,7 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
 // step share one publish and the live columns fill whole warps); a CTA's last instances past the
 // batch repeat the batch's last instance and write nothing.
 #ifndef MAYO_TAIL_G
-#define MAYO_TAIL_G 2
+#define MAYO_TAIL_G 1
 #endif
 template <int SET>
 struct TailShape {

@@ -136,9 +136,8 @@ def test_product_stall_falls_back_to_engine(cuda, injection, s):
     epk = _dev(np.frombuffer(O.expandpk(s, pk), np.uint8))
     lens = rng.integers(0, 400, n).astype(np.uint32)
     msgs = [rng.integers(0, 256, int(k), dtype=np.uint8).tobytes() for k in lens]
-    if s != 2:
-        msgs[7] = _reject_msg(s)
-        lens[7] = 32
+    msgs[7] = _reject_msg(s)
+    lens[7] = 32
     offs = np.concatenate([[0], np.cumsum(lens[:-1])]).astype(np.int64)
     d_msg = _dev(np.frombuffer(b"".join(msgs) + b"\0", np.uint8))
     d_off, d_len = _dev(offs), _dev(lens.view(np.int32))

@@ -64,7 +64,7 @@ def test_sign_verify_golden(mset):
         assert list(G.verify(m, epk, msgs, bad)) == ent["verify_plain_bad"]
 
 
-@pytest.mark.parametrize("s", [1, 3, 5])
+@pytest.mark.parametrize("s", [1, 2, 3, 5])
 def test_rejection_retry_golden(s, cuda):
     """Messages whose first attempt is singular (attempts == 2): the retry path."""
     m = Mayo(s)

@@ -40,11 +40,11 @@ def build_case(rng):
         esk = np.stack([np.frombuffer(O.expandsk(s, k), np.uint8) for k in (sk0, seed1)])
         epk = np.stack([np.frombuffer(O.expandpk(s, k), np.uint8) for k in (pk0, pk1)])
         msgs = rng.integers(0, 256, (4, MLEN), dtype=np.uint8)
-        if s != 2:  # first attempt singular under key 0 (tests/golden/rejection_msgs.json)
-            g = json.load(open(os.path.join(GOLDEN, f"ref_mayo{s}.json")))["rejection"]
-            msgs[0] = np.frombuffer(hashlib.shake_256(f"reject-search/{s}/{g['indices'][0]}".encode())
-                                    .digest(MLEN), np.uint8)
-            n_retry += 1
+        # first attempt singular under key 0 (tests/golden/rejection_msgs.json)
+        g = json.load(open(os.path.join(GOLDEN, f"ref_mayo{s}.json")))["rejection"]
+        msgs[0] = np.frombuffer(hashlib.shake_256(f"reject-search/{s}/{g['indices'][0]}".encode())
+                                .digest(MLEN), np.uint8)
+        n_retry += 1
         sig_want = np.stack([np.frombuffer(O.sign(s, esk[i % 2].tobytes(), msgs[i].tobytes())[0], np.uint8)
                              for i in range(4)])
         vsig = sig_want.copy()
@@ -88,7 +88,7 @@ def test_queue_mixed_sets_and_ops(cuda):
     assert st["requeued_signs"] == n_retry
     assert st["finished"] == st["published"] == len(entries) + n_retry
     for (s, op), p in st["per_bucket"].items():
-        assert p["published"] == 3 + (op != Q.OP_KEYPAIR) + (op == Q.OP_SIGN and s != 2), (s, op)
+        assert p["published"] == 3 + (op != Q.OP_KEYPAIR) + (op == Q.OP_SIGN), (s, op)
     check(operands, expect)
 
 

@@ -96,7 +96,7 @@ def test_sign_verify_golden(s):
         assert list(O.verify_batch(s, epk, msgs, bad)) == ent["verify_bad"]
 
 
-@pytest.mark.parametrize("s", [1, 3, 5])
+@pytest.mark.parametrize("s", [1, 2, 3, 5])
 def test_rejection_path_golden(s):
     rej = golden(s)["rejection"]
     sk, _ = O.keypair(s, 0, 0)
