@@ -20,10 +20,6 @@
 
 #include "common.cuh"
 
-#ifndef MAYO_ENGINE_X4
-#define MAYO_ENGINE_X4 0
-#endif
-
 namespace mayo {
 
 // Packed bytes [p, p + n) (n <= 16) of an m-vector group as four LE words, touching only
@@ -113,7 +109,10 @@ struct EngineSmem {
 //   __device__ int count(int r) const;                  entries in row r
 //   __device__ const uint8_t *entry(int r, int e) const; packed entry (nullptr -> zero vector)
 //   __device__ int col(int r, int e) const;             scalar column of entry e
-template <int SET, int J, int R>
+// X4: row products with four partial sums (row_product_x4, measured 3-4 % faster keypair, sign
+// and verify at 1,024 instances, 4 % on the mixed queue); off where a kernel's register budget
+// leaves no room for the twelve extra live registers.
+template <int SET, int J, int R, bool X4 = true>
 struct Engine {
     using S = Set<SET>;
     static constexpr int W = S::W;
@@ -156,9 +155,7 @@ struct Engine {
     // T_j[r] for this thread's (j, w) over row r = r0 + rs (call only when active and r < nrows).
     template <class Rows>
     __device__ __forceinline__ G4 row_product(const Rows &rows, int r) const {
-#if MAYO_ENGINE_X4
-        return row_product_x4(rows, r);
-#else
+        if constexpr (X4) return row_product_x4(rows, r);
         G4 acc = g4_zero();
         const int cnt = rows.count(r);
         const uint4 *bp = bs + (size_t)rs * MAXE * W + w;
@@ -171,7 +168,6 @@ struct Engine {
             g4_madd(acc, v, m);
         }
         return acc;
-#endif
     }
     // The same with four partial sums, one per power of x, folded once at the end of the row
     // (g4x4_madd): three XORs fewer per entry, twelve more live registers.

@@ -99,7 +99,9 @@ __device__ __forceinline__ void verify_instance(uint8_t *smem, int tid, const ui
         }
         bar_sync(1, NC);
 
-        Engine<SET, J, R> eng;
+        // MAYO_3's verify is held to 80 registers for 6 CTAs per SM: the four-partial-sum row
+        // product spills there (1.48 M against 1.51 M distinct-key verify/s), so it keeps g4_madd
+        Engine<SET, J, R, SET != 3> eng;
         eng.setup(masks, bs, tid);
         const VerifyRows<SET> rows{epk, epk + S::p1, epk + S::p};
         G4 X[J];
