@@ -505,6 +505,17 @@ def run_ours(args, dist: Dist):
     else:
         raise SystemExit(f"unknown workload {args.workload}")
 
+    tuned = None
+    if wl["kind"] == "shared_sign_verify":
+        # block shapes of the shared-key calls (hash CTA threads, sign-tail instances per CTA),
+        # timed on this GPU by the autotuner (cached per GPU, library build, set and batch)
+        from cumayo_b200 import autotune as AT
+        tuned = AT.tune_shared(m, lambda: [fn() for _, fn in phases], batch, flush=lambda: flush.fill_(1))
+        cfg["shape"] = {"hash_threads": tuned["hash_threads"], "tail_instances": tuned["tail_instances"],
+                        "chosen_by": "cumayo_b200.autotune.tune_shared",
+                        "trials_ms": {f"{t['hash_threads']}x{t['tail_instances']}": round(t["ms"], 4)
+                                      for t in tuned.get("trials", [])}}
+
     def step():
         flush.fill_(1)
         for _, fn in phases:

@@ -105,10 +105,19 @@ def lib() -> ctypes.CDLL:
         L.mayo_b200_shared_timing.argtypes = [ctypes.c_int]
         L.mayo_b200_shared_timing_read.restype = ctypes.c_int
         L.mayo_b200_shared_timing_read.argtypes = [ctypes.POINTER(ctypes.c_float)]
+        L.mayo_b200_shared_set_shape.restype = ctypes.c_int
+        L.mayo_b200_shared_set_shape.argtypes = [ctypes.c_int, ctypes.POINTER(SharedShape)]
+        L.mayo_b200_shared_get_shape.restype = ctypes.c_int
+        L.mayo_b200_shared_get_shape.argtypes = [ctypes.c_int, ctypes.POINTER(SharedShape)]
         L.mayo_b200_test_inject.restype = ctypes.c_int
         L.mayo_b200_test_inject.argtypes = [ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32]
         _lib = L
     return _lib
+
+
+class SharedShape(ctypes.Structure):
+    """mayo_b200_shared_shape: launch shape of a set's shared-key calls."""
+    _fields_ = [("hash_threads", ctypes.c_uint32), ("tail_instances", ctypes.c_uint32)]
 
 
 INJECT_NONE, INJECT_QUEUE_LOST_PUSH, INJECT_PRODUCT_STALL = 0, 1, 2
@@ -343,6 +352,17 @@ class Mayo:
                                              _ptr(ws), batch, _stream(stream)), "verify_shared")
 
     SHARED_KERNELS = ("hash", "key_tiles", "product", "tail", "fixup")
+
+    def set_shared_shape(self, hash_threads: int = 0, tail_instances: int = 0) -> None:
+        """Launch shape of this set's sign_shared / verify_shared calls (process-wide): threads
+        per CTA of the hash kernels, signatures per sign-tail CTA; 0 = default."""
+        _check(lib().mayo_b200_shared_set_shape(self.set, ctypes.byref(SharedShape(hash_threads, tail_instances))),
+               "shared_set_shape")
+
+    def shared_shape(self) -> dict:
+        sh = SharedShape()
+        _check(lib().mayo_b200_shared_get_shape(self.set, ctypes.byref(sh)), "shared_get_shape")
+        return {"hash_threads": int(sh.hash_threads), "tail_instances": int(sh.tail_instances)}
 
     @staticmethod
     def shared_timing(enable: bool) -> None:

@@ -1,11 +1,17 @@
-"""Autotuner for the persistent work queue.
+"""Autotuners: the persistent work queue's launch shapes and the shared-key path's block shapes.
 
-For a given queue (operands already set) it times candidate launch shapes on the actual GPU with
-CUDA events — the resident CTAs per SM of each (set, op) bucket's kernel and the order in which
-the bucket kernels are launched (the first one launched takes the SMs first, the later ones fill
-in as its CTAs finish) — and keeps the fastest.  Results are cached per (GPU name, SMs, workload
-signature) in a JSON file (MAYO_B200_TUNE_CACHE, default ~/.cache/mayo_b200/autotune.json) so
-later runs skip the search.
+tune_queue: for a given queue (operands already set) it times candidate launch shapes on the
+actual GPU with CUDA events — the resident CTAs per SM of each (set, op) bucket's kernel and the
+order in which the bucket kernels are launched (the first one launched takes the SMs first, the
+later ones fill in as its CTAs finish) — and keeps the fastest.
+
+tune_shared: for one set's sign_shared + verify_shared on a given batch it times the block shapes
+the library can run — threads per CTA of the thread-per-instance hash kernels (32..256) and
+signatures per sign-tail CTA (1, or 2 with the instances' elimination columns interleaved) — and
+sets the fastest (mayo_b200_shared_set_shape).
+
+Results are cached per (GPU name, SMs, workload) in a JSON file (MAYO_B200_TUNE_CACHE, default
+~/.cache/mayo_b200/autotune.json) so later runs skip the search.
 """
 from __future__ import annotations
 
@@ -106,4 +112,57 @@ def tune_queue(q: "Q.Queue", items: np.ndarray, repeats: int = 2, use_cache: boo
     cps = {tuple(int(x) for x in k.split("/")): c for k, c in best["ctas_per_sm"].items()}
     q.shape = Q.Shape(sms=q.shape.sms, ctas_per_sm=clamp_shape(cps, per_max),
                       launch_order=[tuple(b) for b in best["order_buckets"]])
+    return best
+
+
+SHARED_CANDIDATES = [(h, g) for g in (1, 2) for h in (32, 64, 128, 256)]
+
+
+def _lib_id() -> str:
+    """Digest of the library file: shapes tuned for one build are not replayed on another."""
+    import hashlib
+    from .api import LIB_PATH
+    try:
+        with open(LIB_PATH, "rb") as f:
+            return hashlib.sha1(f.read()).hexdigest()[:12]
+    except OSError:
+        return "none"
+
+
+def tune_shared(m, run, batch: int, repeats: int = 3, flush=None, use_cache: bool = True) -> dict:
+    """Pick the shared-key block shape of m's set for `run()` (a callable that issues the
+    sign_shared / verify_shared work being tuned, on the current stream) at `batch` instances.
+    `flush()`, when given, runs before every timed call (an L2 flush).  Sets the winner."""
+    import torch
+    dev = torch.cuda.current_device()
+    props = torch.cuda.get_device_properties(dev)
+    key = f"{props.name}|sms={props.multi_processor_count}|lib={_lib_id()}|shared:set={m.set}|batch={batch}"
+    cache = _load() if use_cache else {}
+    if key in cache:
+        best = cache[key]
+    else:
+        trials = []
+        for h, g in SHARED_CANDIDATES:
+            try:
+                m.set_shared_shape(h, g)
+            except Exception:  # a shape this set's kernels cannot take (shared memory)
+                continue
+            run()
+            torch.cuda.synchronize()
+            ms = []
+            for _ in range(repeats):
+                if flush is not None:
+                    flush()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                run()
+                b.record()
+                torch.cuda.synchronize()
+                ms.append(a.elapsed_time(b))
+            trials.append({"hash_threads": h, "tail_instances": g, "ms": min(ms)})
+        best = dict(min(trials, key=lambda t: t["ms"]), trials=trials)
+        cache[key] = best
+        if use_cache:
+            _store(cache)
+    m.set_shared_shape(best["hash_threads"], best["tail_instances"])
     return best

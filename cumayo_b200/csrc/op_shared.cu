@@ -35,6 +35,8 @@
 //   every instance through the per-instance engine, so results stay correct.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "../../include/mayo_b200.h"
 #include "launch_util.cuh"
 #include "ops.h"
@@ -539,22 +541,22 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
 // SH_TAIL_G instances per CTA (sign_attempt's interleaved elimination: the G pivot owners of a
 // step share one publish and the live columns fill whole warps); a CTA's last instances past the
 // batch repeat the batch's last instance and write nothing.
-#ifndef MAYO_TAIL_G
-#define MAYO_TAIL_G 1
-#endif
-template <int SET>
+// G (instances per CTA) is a runtime choice of the shared-key shape (mayo_b200_shared_set_shape):
+// 1 or 2, the autotuner's candidates.
+template <int SET, int G>
 struct TailShape {
-    static constexpr int G = MAYO_TAIL_G;  // instances per CTA
     static constexpr int NT = SignCfg<SET>::NT * G;
-    static constexpr int MINB = SET == 5 ? 2 : 1;  // MAYO_5: held to a register budget
+    // MAYO_5: 5 CTAs of 160 threads per SM held to a register budget (72 registers)
+    static constexpr int MINB = SET == 5 ? (G == 1 ? 5 : 2) : 1;
+    static constexpr size_t SMEM = (size_t)G * SignCfg<SET, 0, true>::total;
 };
-template <int SET>
-__global__ void __launch_bounds__(TailShape<SET>::NT, TailShape<SET>::MINB)
+template <int SET, int G>
+__global__ void __launch_bounds__(TailShape<SET, G>::NT, TailShape<SET, G>::MINB)
     sign_shared_tail_kernel(const uint8_t *esk, uint8_t *sig, size_t sig_stride, const uint8_t *wsi, size_t wsi_stride,
                             const uint4 *planes, const uint4 *opl, uint32_t *ctl, uint32_t *retry, uint32_t batch) {
     using P = SharedProb<SET, false>;
     using C = SignCfg<SET, 0, true>;
-    constexpr int G = TailShape<SET>::G, NT = C::NT;
+    constexpr int NT = C::NT;
     extern __shared__ __align__(16) uint8_t smem0[];
     if (ctl[0]) return;  // the product gave up: the fix-up kernel signs everything
     const int T = threadIdx.x, g = T / NT, tid = T % NT;
@@ -733,6 +735,14 @@ static void tmark(cudaStream_t st) {
     if (tl_tm.on && tl_tm.ready && tl_tm.n < 6) cudaEventRecord(tl_tm.ev[tl_tm.n++], st);
 }
 
+// ---- runtime shape of the shared-key path, per parameter set (mayo_b200_shared_set_shape) ----
+struct SharedShape {
+    std::atomic<int> hash_nt{HASH_NT};  // threads per CTA of the thread-per-instance hash kernels
+    std::atomic<int> tail_g{1};         // instances per sign-tail CTA
+};
+SharedShape g_shape[4];
+static int shape_index(int set) { return set == 1 ? 0 : set == 2 ? 1 : set == 3 ? 2 : set == 5 ? 3 : -1; }
+
 // ---- launchers ----
 template <int SET, bool VERIFY>
 static int launch_product(const uint8_t *key, const uint8_t *vec, size_t vec_stride, uint8_t *ws, size_t batch,
@@ -769,19 +779,29 @@ static int sign_shared_t(const SignIO &io0, uint8_t *ws, size_t batch, cudaStrea
     io.ws_stride = WSL::inst;
     tl_tm.n = 0;
     tmark(st);
+    const SharedShape &shp = g_shape[shape_index(SET)];
+    const int hnt = shp.hash_nt.load(std::memory_order_relaxed), tg = shp.tail_g.load(std::memory_order_relaxed);
     const uint32_t *order = launch_hash_order<SET, false>(io.m, ws, batch, st);
-    int rc = launch_sign_hash(SET, io, batch, st, order);
+    int rc = launch_sign_hash(SET, io, batch, st, order, hnt);
     tmark(st);
     if (rc != ST_OK) return rc;
     rc = launch_product<SET, false>(io.esk, io.ws + SignWs<SET>::vr, io.ws_stride, ws, batch, st);
     if (rc != ST_OK) return rc;
     uint32_t *ctl = reinterpret_cast<uint32_t *>(ws);
     uint32_t *retry = reinterpret_cast<uint32_t *>(ws + WSL::retry_off(batch));
-    constexpr int TG = TailShape<SET>::G;
-    if (!set_smem_attr(sign_shared_tail_kernel<SET>, TG * CT::total)) return ST_CUDA;
-    sign_shared_tail_kernel<SET><<<(unsigned)((batch + TG - 1) / TG), TailShape<SET>::NT, TG * CT::total, st>>>(
-        io.esk, io.sig, io.sig_stride, io.ws, io.ws_stride, reinterpret_cast<const uint4 *>(ws + WSL::planes_off(batch)),
-        reinterpret_cast<const uint4 *>(ws + WSL::op_off()), ctl, retry, (uint32_t)batch);
+    const uint4 *planes = reinterpret_cast<const uint4 *>(ws + WSL::planes_off(batch));
+    const uint4 *opl = reinterpret_cast<const uint4 *>(ws + WSL::op_off());
+    if (tg == 2) {
+        using TS = TailShape<SET, 2>;
+        if (!set_smem_attr(sign_shared_tail_kernel<SET, 2>, TS::SMEM)) return ST_CUDA;
+        sign_shared_tail_kernel<SET, 2><<<(unsigned)((batch + 1) / 2), TS::NT, TS::SMEM, st>>>(
+            io.esk, io.sig, io.sig_stride, io.ws, io.ws_stride, planes, opl, ctl, retry, (uint32_t)batch);
+    } else {
+        using TS = TailShape<SET, 1>;
+        if (!set_smem_attr(sign_shared_tail_kernel<SET, 1>, TS::SMEM)) return ST_CUDA;
+        sign_shared_tail_kernel<SET, 1><<<(unsigned)batch, TS::NT, TS::SMEM, st>>>(
+            io.esk, io.sig, io.sig_stride, io.ws, io.ws_stride, planes, opl, ctl, retry, (uint32_t)batch);
+    }
     tmark(st);
     if (!set_smem_attr(sign_shared_fix_kernel<SET>, CF::total)) return ST_CUDA;
     sign_shared_fix_kernel<SET><<<fix_grid(batch), CF::NT, CF::total, st>>>(
@@ -802,8 +822,9 @@ static int verify_shared_t(const VerifyIO &io0, uint8_t *ws, size_t batch, cudaS
     tl_tm.n = 0;
     tmark(st);
     const uint32_t *order = launch_hash_order<SET, true>(io.m, ws, batch, st);
-    verify_hash_kernel<SET><<<(unsigned)((batch + HASH_NT - 1) / HASH_NT), HASH_NT, 0, st>>>(io, tws, WSL::inst,
-                                                                                       (uint32_t)batch, order);
+    const int hnt = g_shape[shape_index(SET)].hash_nt.load(std::memory_order_relaxed);
+    verify_hash_kernel<SET><<<(unsigned)((batch + hnt - 1) / hnt), hnt, 0, st>>>(io, tws, WSL::inst, (uint32_t)batch,
+                                                                             order);
     tmark(st);
     int rc = launch_product<SET, true>(io.epk, io.sig, io.sig_stride, ws, batch, st);
     if (rc != ST_OK) return rc;
@@ -844,6 +865,37 @@ int shared_timing_read(float *ms) {
     if (cudaEventSynchronize(tl_tm.ev[5]) != cudaSuccess) return ST_CUDA;
     for (int i = 0; i < 5; i++)
         if (cudaEventElapsedTime(&ms[i], tl_tm.ev[i], tl_tm.ev[i + 1]) != cudaSuccess) return ST_CUDA;
+    return ST_OK;
+}
+
+// Shared memory a sign-tail CTA of g instances needs (0 for a bad set).
+static size_t tail_smem(int set, int g) {
+    switch (set) {
+        case 1: return (size_t)g * SignCfg<1, 0, true>::total;
+        case 2: return (size_t)g * SignCfg<2, 0, true>::total;
+        case 3: return (size_t)g * SignCfg<3, 0, true>::total;
+        case 5: return (size_t)g * SignCfg<5, 0, true>::total;
+        default: return 0;
+    }
+}
+
+int shared_set_shape(int set, int hash_nt, int tail_g) {
+    const int si = shape_index(set);
+    if (si < 0) return ST_BAD_SET;
+    if (hash_nt == 0) hash_nt = HASH_NT;
+    if (tail_g == 0) tail_g = 1;
+    if (hash_nt < 32 || hash_nt > 1024 || hash_nt % 32 || (tail_g != 1 && tail_g != 2)) return ST_BAD_ARG;
+    if (tail_smem(set, tail_g) > SH_SMEM_MAX) return ST_BAD_ARG;
+    g_shape[si].hash_nt.store(hash_nt);
+    g_shape[si].tail_g.store(tail_g);
+    return ST_OK;
+}
+
+int shared_get_shape(int set, int *hash_nt, int *tail_g) {
+    const int si = shape_index(set);
+    if (si < 0) return ST_BAD_SET;
+    *hash_nt = g_shape[si].hash_nt.load();
+    *tail_g = g_shape[si].tail_g.load();
     return ST_OK;
 }
 

@@ -90,15 +90,15 @@ static int sign_t(const SignIO &io, size_t batch, cudaStream_t st) {
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
 }
 
-int launch_sign_hash(int set, const SignIO &io, size_t batch, cudaStream_t st, const uint32_t *order) {
+int launch_sign_hash(int set, const SignIO &io, size_t batch, cudaStream_t st, const uint32_t *order, int nt) {
     if (batch == 0) return ST_OK;
-    const unsigned g = (unsigned)((batch + HASH_NT - 1) / HASH_NT);
+    const unsigned g = (unsigned)((batch + nt - 1) / nt);
     const uint32_t b = (uint32_t)batch;
     switch (set) {
-        case 1: sign_hash_kernel<1><<<g, HASH_NT, 0, st>>>(io, b, order); break;
-        case 2: sign_hash_kernel<2><<<g, HASH_NT, 0, st>>>(io, b, order); break;
-        case 3: sign_hash_kernel<3><<<g, HASH_NT, 0, st>>>(io, b, order); break;
-        case 5: sign_hash_kernel<5><<<g, HASH_NT, 0, st>>>(io, b, order); break;
+        case 1: sign_hash_kernel<1><<<g, nt, 0, st>>>(io, b, order); break;
+        case 2: sign_hash_kernel<2><<<g, nt, 0, st>>>(io, b, order); break;
+        case 3: sign_hash_kernel<3><<<g, nt, 0, st>>>(io, b, order); break;
+        case 5: sign_hash_kernel<5><<<g, nt, 0, st>>>(io, b, order); break;
         default: return ST_BAD_SET;
     }
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;

@@ -73,7 +73,8 @@ struct VerifyIO {
 int launch_sign_io(int set, const SignIO &io, size_t batch, cudaStream_t st);
 // Only the hash stage of sign (digest, salt, t, V || r for ctr 0 into io.ws).
 // order (optional, batch entries): thread i hashes instance order[i]
-int launch_sign_hash(int set, const SignIO &io, size_t batch, cudaStream_t st, const uint32_t *order = nullptr);
+int launch_sign_hash(int set, const SignIO &io, size_t batch, cudaStream_t st, const uint32_t *order = nullptr,
+                     int nt = HASH_NT);
 int launch_verify_io(int set, const VerifyIO &io, size_t batch, cudaStream_t st);
 // Workspace bytes per instance used by sign (digest, salt, t, V || r).
 size_t sign_ws_bytes(int set);
@@ -83,6 +84,9 @@ int launch_sign_shared(int set, const SignIO &io, uint8_t *ws, size_t batch, cud
 int launch_verify_shared(int set, const VerifyIO &io, uint8_t *ws, size_t batch, cudaStream_t st);
 int shared_timing(int enable);
 int shared_timing_read(float *ms);
+// Runtime shape of the shared-key path per set: hash-kernel CTA threads, sign-tail instances per CTA.
+int shared_set_shape(int set, int hash_nt, int tail_g);
+int shared_get_shape(int set, int *hash_nt, int *tail_g);
 
 // Status plumbing of the C-ABI (capi.cu): a failed CUDA call or launch is recorded as the calling
 // thread's last CUDA error (mayo_b200_last_cuda_error) and reported as ST_CUDA.  api_launch_rc

@@ -190,6 +190,18 @@ MAYO_B200_API size_t mayo_b200_verify_shared_ws_bytes(int set, size_t batch);
  * call and gives the milliseconds of its kernels: [0] hash, [1] key tiles, [2] tensor-core
  * product, [3] per-instance tail, [4] fix-up.  MAYO_B200_ERR_ARG if no call was recorded. */
 MAYO_B200_API int mayo_b200_shared_timing(int enable);
+/* Launch shape of the shared-key calls of one parameter set, process-wide (set it before the
+ * calls it should apply to; calls already issued keep theirs).  hash_threads: threads per CTA
+ * of the thread-per-instance hash kernels (a multiple of 32, 32..1024; 0 = 64); tail_instances:
+ * signatures per CTA of the sign tail (1 or 2; 0 = 1; with 2 the two instances' elimination
+ * columns are interleaved over the CTA's warps).  Results do not depend on the shape;
+ * cumayo_b200.autotune times the candidates.  MAYO_B200_ERR_ARG for a shape out of range or
+ * one whose CTA would not fit in shared memory; shape NULL = the defaults. */
+typedef struct mayo_b200_shared_shape {
+    uint32_t hash_threads, tail_instances;
+} mayo_b200_shared_shape;
+MAYO_B200_API int mayo_b200_shared_set_shape(int set, const mayo_b200_shared_shape *shape);
+MAYO_B200_API int mayo_b200_shared_get_shape(int set, mayo_b200_shared_shape *shape);
 MAYO_B200_API int mayo_b200_shared_timing_read(float *ms);
 MAYO_B200_API int mayo_b200_verify_shared(int set, const uint8_t *epk, const uint8_t *msgs, const uint64_t *msg_off,
                                           const uint32_t *msg_len, size_t msg_stride, size_t mlen, const uint8_t *sig,

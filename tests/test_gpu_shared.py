@@ -119,3 +119,40 @@ def test_shared_key_large_batch(cuda, s):
     expect = np.zeros(n, np.uint8)
     expect[::7] = 1
     assert res.cpu().numpy().tolist() == expect.tolist()
+
+
+@pytest.mark.parametrize("s", [1, 2, 3, 5])
+def test_shared_key_block_shapes(cuda, s):
+    """Every block shape the autotuner may choose (hash CTA threads, sign-tail instances per CTA)
+    gives the bytes of the per-instance path, also for an odd batch (a last CTA half empty)."""
+    import torch
+    m = Mayo(s)
+    z = m.sizes
+    rng = np.random.default_rng(300 + s)
+    n = 301
+    sk, pk = O.keypair(s, 0, 0)
+    esk = _dev(np.frombuffer(O.expandsk(s, sk), np.uint8))
+    epk = _dev(np.frombuffer(O.expandpk(s, pk), np.uint8))
+    msgs = _messages(s, n, rng)
+    lens = np.array([len(x) for x in msgs], np.uint32)
+    offs = np.concatenate([[0], np.cumsum(lens[:-1])]).astype(np.int64)
+    d_msg, d_off, d_len = _dev(np.frombuffer(b"".join(msgs) + b"\0", np.uint8)), _dev(offs), _dev(lens.view(np.int32))
+    sig_ref = torch.zeros(n * z.sig_bytes, dtype=torch.uint8, device="cuda")
+    ws_ref = torch.zeros(n * m.sign_ws_bytes(), dtype=torch.uint8, device="cuda")
+    m.sign_many(esk, d_msg, sig_ref, ws_ref, n, msg_off=d_off, msg_len=d_len)
+    res_ref = torch.full((n,), 0xEE, dtype=torch.uint8, device="cuda")
+    m.verify_many(epk, d_msg, sig_ref, res_ref, n, msg_off=d_off, msg_len=d_len)
+    ws = torch.zeros(max(m.sign_shared_ws_bytes(n), m.verify_shared_ws_bytes(n)), dtype=torch.uint8, device="cuda")
+    try:
+        for h, g in ((32, 2), (128, 2), (256, 1), (64, 1)):
+            m.set_shared_shape(h, g)
+            assert m.shared_shape() == {"hash_threads": h, "tail_instances": g}
+            sig = torch.zeros_like(sig_ref)
+            m.sign_shared(esk, d_msg, sig, ws, n, msg_off=d_off, msg_len=d_len)
+            res = torch.full((n,), 0xEE, dtype=torch.uint8, device="cuda")
+            m.verify_shared(epk, d_msg, sig, res, ws, n, msg_off=d_off, msg_len=d_len)
+            torch.cuda.synchronize()
+            assert torch.equal(sig, sig_ref), (h, g)
+            assert torch.equal(res, res_ref) and int(res.sum()) == 0, (h, g)
+    finally:
+        m.set_shared_shape(0, 0)
