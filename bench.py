@@ -1525,7 +1525,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--batch", type=int, default=0)
-    ap.add_argument("--inflight", type=int, default=4, help="c5: batches on the GPU at once")
+    ap.add_argument("--inflight", type=int, default=6, help="c5: batches on the GPU at once")
     ap.add_argument("--e2e-chunks", type=int, default=8,
                     help="c2: sub-batches (one stream each) of the end-to-end measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")

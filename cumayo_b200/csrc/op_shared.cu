@@ -547,7 +547,10 @@ template <int SET, int G>
 struct TailShape {
     static constexpr int NT = SignCfg<SET>::NT * G;
     // MAYO_5: 5 CTAs of 160 threads per SM held to a register budget (72 registers)
-    static constexpr int MINB = SET == 5 ? (G == 1 ? 5 : 2) : 1;
+#ifndef MAYO_TAIL2_MINB
+#define MAYO_TAIL2_MINB 1
+#endif
+    static constexpr int MINB = SET == 5 ? (G == 1 ? 5 : 2) : (G == 2 ? MAYO_TAIL2_MINB : 1);
     static constexpr size_t SMEM = (size_t)G * SignCfg<SET, 0, true>::total;
 };
 template <int SET, int G>
