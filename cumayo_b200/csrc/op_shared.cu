@@ -547,10 +547,10 @@ template <int SET, int G>
 struct TailShape {
     static constexpr int NT = SignCfg<SET>::NT * G;
     // MAYO_5: 5 CTAs of 160 threads per SM held to a register budget (72 registers)
-#ifndef MAYO_TAIL2_MINB
-#define MAYO_TAIL2_MINB 1
-#endif
-    static constexpr int MINB = SET == 5 ? (G == 1 ? 5 : 2) : (G == 2 ? MAYO_TAIL2_MINB : 1);
+    // MAYO_2 with two instances per CTA: 5 CTAs per SM (10 signatures in flight, 48 registers)
+    // beat 4 (1.737 against 1.889 ms at 65,536) and 6 (1.777 ms); the elimination's per-step
+    // chain needs the instances in flight more than the registers
+    static constexpr int MINB = SET == 5 ? (G == 1 ? 5 : 2) : (SET == 2 && G == 2 ? 5 : 1);
     static constexpr size_t SMEM = (size_t)G * SignCfg<SET, 0, true>::total;
 };
 template <int SET, int G>
