@@ -7,7 +7,7 @@ later ones fill in as its CTAs finish) — and keeps the fastest.
 
 tune_shared: for one set's sign_shared + verify_shared on a given batch it times the block shapes
 the library can run — threads per CTA of the thread-per-instance hash kernels (32..256) and
-signatures per sign-tail CTA (1, or 2 with the instances' elimination columns interleaved) — and
+signatures per sign-tail CTA (1, or 2 or 4 with the instances' elimination columns interleaved) — and
 sets the fastest (mayo_b200_shared_set_shape).
 
 Results are cached per (GPU name, SMs, workload) in a JSON file (MAYO_B200_TUNE_CACHE, default
@@ -115,7 +115,7 @@ def tune_queue(q: "Q.Queue", items: np.ndarray, repeats: int = 2, use_cache: boo
     return best
 
 
-SHARED_CANDIDATES = [(h, g) for g in (1, 2) for h in (32, 64, 128, 256)]
+SHARED_CANDIDATES = [(h, g) for g in (1, 2, 4) for h in (32, 64, 128, 256)]
 
 
 def _lib_id() -> str:

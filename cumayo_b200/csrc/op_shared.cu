@@ -542,15 +542,16 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
 // step share one publish and the live columns fill whole warps); a CTA's last instances past the
 // batch repeat the batch's last instance and write nothing.
 // G (instances per CTA) is a runtime choice of the shared-key shape (mayo_b200_shared_set_shape):
-// 1 or 2, the autotuner's candidates.
+// 1, 2 or 4, the autotuner's candidates (4 only where the CTA fits in shared memory).
 template <int SET, int G>
 struct TailShape {
     static constexpr int NT = SignCfg<SET>::NT * G;
     // MAYO_5: 5 CTAs of 160 threads per SM held to a register budget (72 registers)
-    // MAYO_2 with two instances per CTA: 5 CTAs per SM (10 signatures in flight, 48 registers)
-    // beat 4 (1.737 against 1.889 ms at 65,536) and 6 (1.777 ms); the elimination's per-step
-    // chain needs the instances in flight more than the registers
-    static constexpr int MINB = SET == 5 ? (G == 1 ? 5 : 2) : (SET == 2 && G == 2 ? 5 : 1);
+    // MAYO_2: the elimination's per-step chain needs signatures in flight more than registers.
+    // At 65,536: G = 1, 9 CTAs per SM (56 registers) 1.866 ms; G = 2 with 5 CTAs (48 registers)
+    // 1.739 ms (4 CTAs: 1.889, 6: 1.777); G = 4 with 3 CTAs (40 registers, 12 signatures per SM)
+    // 1.661 ms (2 CTAs: 2.055)
+    static constexpr int MINB = SET == 5 ? (G == 1 ? 5 : 2) : (SET == 2 ? (G == 1 ? 1 : G == 2 ? 5 : 3) : 1);
     static constexpr size_t SMEM = (size_t)G * SignCfg<SET, 0, true>::total;
 };
 template <int SET, int G>
@@ -771,10 +772,24 @@ static int launch_product(const uint8_t *key, const uint8_t *vec, size_t vec_str
 
 static unsigned fix_grid(size_t batch) { return (unsigned)(batch < SH_FIX_CTAS ? batch : SH_FIX_CTAS); }
 
+// The sign tail with G instances per CTA (ST_BAD_ARG where such a CTA does not fit).
+template <int SET, int G>
+static int launch_sign_tail(const SignIO &io, const uint4 *planes, const uint4 *opl, uint32_t *ctl, uint32_t *retry,
+                            size_t batch, cudaStream_t st) {
+    using TS = TailShape<SET, G>;
+    if constexpr (TS::SMEM > SH_SMEM_MAX) {
+        return ST_BAD_ARG;
+    } else {
+        if (!set_smem_attr(sign_shared_tail_kernel<SET, G>, TS::SMEM)) return ST_CUDA;
+        sign_shared_tail_kernel<SET, G><<<(unsigned)((batch + G - 1) / G), TS::NT, TS::SMEM, st>>>(
+            io.esk, io.sig, io.sig_stride, io.ws, io.ws_stride, planes, opl, ctl, retry, (uint32_t)batch);
+        return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
+    }
+}
+
 template <int SET>
 static int sign_shared_t(const SignIO &io0, uint8_t *ws, size_t batch, cudaStream_t st) {
     using WSL = SharedWs<SET, false>;
-    using CT = SignCfg<SET, 0, true>;
     using CF = SignCfg<SET>;
     SignIO io = io0;
     io.esk_stride = 0;
@@ -794,17 +809,10 @@ static int sign_shared_t(const SignIO &io0, uint8_t *ws, size_t batch, cudaStrea
     uint32_t *retry = reinterpret_cast<uint32_t *>(ws + WSL::retry_off(batch));
     const uint4 *planes = reinterpret_cast<const uint4 *>(ws + WSL::planes_off(batch));
     const uint4 *opl = reinterpret_cast<const uint4 *>(ws + WSL::op_off());
-    if (tg == 2) {
-        using TS = TailShape<SET, 2>;
-        if (!set_smem_attr(sign_shared_tail_kernel<SET, 2>, TS::SMEM)) return ST_CUDA;
-        sign_shared_tail_kernel<SET, 2><<<(unsigned)((batch + 1) / 2), TS::NT, TS::SMEM, st>>>(
-            io.esk, io.sig, io.sig_stride, io.ws, io.ws_stride, planes, opl, ctl, retry, (uint32_t)batch);
-    } else {
-        using TS = TailShape<SET, 1>;
-        if (!set_smem_attr(sign_shared_tail_kernel<SET, 1>, TS::SMEM)) return ST_CUDA;
-        sign_shared_tail_kernel<SET, 1><<<(unsigned)batch, TS::NT, TS::SMEM, st>>>(
-            io.esk, io.sig, io.sig_stride, io.ws, io.ws_stride, planes, opl, ctl, retry, (uint32_t)batch);
-    }
+    rc = tg == 4 ? launch_sign_tail<SET, 4>(io, planes, opl, ctl, retry, batch, st)
+         : tg == 2 ? launch_sign_tail<SET, 2>(io, planes, opl, ctl, retry, batch, st)
+                   : launch_sign_tail<SET, 1>(io, planes, opl, ctl, retry, batch, st);
+    if (rc != ST_OK) return rc;
     tmark(st);
     if (!set_smem_attr(sign_shared_fix_kernel<SET>, CF::total)) return ST_CUDA;
     sign_shared_fix_kernel<SET><<<fix_grid(batch), CF::NT, CF::total, st>>>(
@@ -887,7 +895,7 @@ int shared_set_shape(int set, int hash_nt, int tail_g) {
     if (si < 0) return ST_BAD_SET;
     if (hash_nt == 0) hash_nt = HASH_NT;
     if (tail_g == 0) tail_g = 1;
-    if (hash_nt < 32 || hash_nt > 1024 || hash_nt % 32 || (tail_g != 1 && tail_g != 2)) return ST_BAD_ARG;
+    if (hash_nt < 32 || hash_nt > 1024 || hash_nt % 32 || (tail_g != 1 && tail_g != 2 && tail_g != 4)) return ST_BAD_ARG;
     if (tail_smem(set, tail_g) > SH_SMEM_MAX) return ST_BAD_ARG;
     g_shape[si].hash_nt.store(hash_nt);
     g_shape[si].tail_g.store(tail_g);
