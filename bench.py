@@ -67,10 +67,11 @@ KERNEL_ROOF_DEF = {
     "hbm": "algorithmic bytes read + written / kernel time; peak = measured copy bandwidth",
 }
 # DRAM bytes per instance (dram__bytes_read.sum + dram__bytes_write.sum of one launch / its
-# instances) from one ncu capture of the MAYO_2 shared-key kernels at 16,384 instances
-# (profiles/sign_tail_mayo2_shared_b16384.md, profiles/product_gemm_mayo2_shared_b16384.md);
+# instances) from ncu captures of the MAYO_2 shared-key kernels at 16,384 instances (the sign
+# tail with four signatures per CTA: profiles/sign_tail_mayo2_shared_b16384.md; the others:
+# profiles/product_gemm_mayo2_shared_b16384.md);
 # the traffic grows in proportion to the instances, so a launch's traffic is this x its batch.
-KERNEL_TRAFFIC_PER_INST = {2: {"sign.tail": 179.689728e6 / 16384, "verify.tail": 177.242624e6 / 16384,
+KERNEL_TRAFFIC_PER_INST = {2: {"sign.tail": (174.092032e6 + 5.284352e6) / 16384, "verify.tail": 177.242624e6 / 16384,
                                "sign.product": 130.477568e6 / 16384, "verify.product": 128.245248e6 / 16384}}
 # The same for verify_kernel<SET> on distinct keys (one capture of 4,096 instances per set,
 # profiles/verify_distinct_mayo3_mayo5_b4096.md): the instance's EPK is read once.
@@ -506,7 +507,11 @@ def run_ours(args, dist: Dist):
         raise SystemExit(f"unknown workload {args.workload}")
 
     tuned = None
-    if wl["kind"] == "shared_sign_verify":
+    if wl["kind"] == "shared_sign_verify" and args.shape:
+        h_, g_ = (int(x) for x in args.shape.lower().split("x"))
+        m.set_shared_shape(h_, g_)
+        cfg["shape"] = {"hash_threads": h_, "tail_instances": g_, "chosen_by": "--shape"}
+    elif wl["kind"] == "shared_sign_verify":
         # block shapes of the shared-key calls (hash CTA threads, sign-tail instances per CTA),
         # timed on this GPU by the autotuner (cached per GPU, library build, set and batch)
         from cumayo_b200 import autotune as AT
@@ -1529,6 +1534,9 @@ def main():
     ap.add_argument("--e2e-chunks", type=int, default=8,
                     help="c2: sub-batches (one stream each) of the end-to-end measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shape", default="",
+                    help="c2: shared-key block shape HASHxTAIL (hash CTA threads x signatures per tail CTA) "
+                         "instead of the autotuner's choice, e.g. 64x4")
     ap.add_argument("--no-per-set", dest="per_set", action="store_false",
                     help="skip the per-set keypair/sign/verify and distinct-key verify figures (default run)")
     ap.add_argument("--int-peak", action="store_true",
