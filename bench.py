@@ -71,7 +71,7 @@ KERNEL_ROOF_DEF = {
 # tail with four signatures per CTA: profiles/sign_tail_mayo2_shared_b16384.md; the others:
 # profiles/product_gemm_mayo2_shared_b16384.md);
 # the traffic grows in proportion to the instances, so a launch's traffic is this x its batch.
-KERNEL_TRAFFIC_PER_INST = {2: {"sign.tail": (174.092032e6 + 5.284352e6) / 16384, "verify.tail": 177.242624e6 / 16384,
+KERNEL_TRAFFIC_PER_INST = {2: {"sign.tail": (174.092288e6 + 4.834816e6) / 16384, "verify.tail": 177.242624e6 / 16384,
                                "sign.product": 130.477568e6 / 16384, "verify.product": 128.245248e6 / 16384}}
 # The same for verify_kernel<SET> on distinct keys (one capture of 4,096 instances per set,
 # profiles/verify_distinct_mayo3_mayo5_b4096.md): the instance's EPK is read once.
@@ -953,6 +953,8 @@ def cpu_baseline(args, gpu: dict | None = None, sample: int | None = None):
     last end-to-end step), reported as `oracle_check`."""
     from oracle import oracle as O
     wl = WORKLOADS[args.workload]
+    if wl["kind"] not in ("shared_sign_verify", "keypair_sign_verify", "distinct_verify"):
+        return None  # mixed queue / serving: no single-set CPU leg
     s = wl["set"]
     P = O.params(s)
     threads = O.max_threads()
