@@ -508,18 +508,20 @@ def run_ours(args, dist: Dist):
 
     tuned = None
     if wl["kind"] == "shared_sign_verify" and args.shape:
-        h_, g_ = (int(x) for x in args.shape.lower().split("x"))
-        m.set_shared_shape(h_, g_)
-        cfg["shape"] = {"hash_threads": h_, "tail_instances": g_, "chosen_by": "--shape"}
+        parts = [int(x) for x in args.shape.lower().split("x")]
+        h_, g_, p_ = (parts + [1, 1, 1])[:3]
+        m.set_shared_shape(h_, g_, p_)
+        cfg["shape"] = {"hash_threads": h_, "tail_instances": g_, "product_ctas": p_, "chosen_by": "--shape"}
     elif wl["kind"] == "shared_sign_verify":
         # block shapes of the shared-key calls (hash CTA threads, sign-tail instances per CTA),
         # timed on this GPU by the autotuner (cached per GPU, library build, set and batch)
         from cumayo_b200 import autotune as AT
         tuned = AT.tune_shared(m, lambda: [fn() for _, fn in phases], batch, flush=lambda: flush.fill_(1))
         cfg["shape"] = {"hash_threads": tuned["hash_threads"], "tail_instances": tuned["tail_instances"],
+                        "product_ctas": tuned.get("product_ctas", 1),
                         "chosen_by": "cumayo_b200.autotune.tune_shared",
-                        "trials_ms": {f"{t['hash_threads']}x{t['tail_instances']}": round(t["ms"], 4)
-                                      for t in tuned.get("trials", [])}}
+                        "trials_ms": {f"{t['hash_threads']}x{t['tail_instances']}x{t.get('product_ctas', 1)}":
+                                      round(t["ms"], 4) for t in tuned.get("trials", [])}}
 
     def step():
         flush.fill_(1)
@@ -1537,8 +1539,8 @@ def main():
                     help="c2: sub-batches (one stream each) of the end-to-end measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shape", default="",
-                    help="c2: shared-key block shape HASHxTAIL (hash CTA threads x signatures per tail CTA) "
-                         "instead of the autotuner's choice, e.g. 64x4")
+                    help="c2: shared-key block shape HASHxTAIL[xPAIR] (hash CTA threads x signatures per tail CTA "
+                         "x CTAs per product tile) instead of the autotuner's choice, e.g. 64x4x2")
     ap.add_argument("--no-per-set", dest="per_set", action="store_false",
                     help="skip the per-set keypair/sign/verify and distinct-key verify figures (default run)")
     ap.add_argument("--int-peak", action="store_true",

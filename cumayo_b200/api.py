@@ -117,7 +117,8 @@ def lib() -> ctypes.CDLL:
 
 class SharedShape(ctypes.Structure):
     """mayo_b200_shared_shape: launch shape of a set's shared-key calls."""
-    _fields_ = [("hash_threads", ctypes.c_uint32), ("tail_instances", ctypes.c_uint32)]
+    _fields_ = [("hash_threads", ctypes.c_uint32), ("tail_instances", ctypes.c_uint32),
+                ("product_ctas", ctypes.c_uint32)]
 
 
 INJECT_NONE, INJECT_QUEUE_LOST_PUSH, INJECT_PRODUCT_STALL = 0, 1, 2
@@ -353,16 +354,18 @@ class Mayo:
 
     SHARED_KERNELS = ("hash", "key_tiles", "product", "tail", "fixup")
 
-    def set_shared_shape(self, hash_threads: int = 0, tail_instances: int = 0) -> None:
+    def set_shared_shape(self, hash_threads: int = 0, tail_instances: int = 0, product_ctas: int = 0) -> None:
         """Launch shape of this set's sign_shared / verify_shared calls (process-wide): threads
-        per CTA of the hash kernels, signatures per sign-tail CTA; 0 = default."""
-        _check(lib().mayo_b200_shared_set_shape(self.set, ctypes.byref(SharedShape(hash_threads, tail_instances))),
-               "shared_set_shape")
+        per CTA of the hash kernels, signatures per sign-tail CTA, CTAs per key-product tile
+        (1 or a CTA pair); 0 = default."""
+        sh = SharedShape(hash_threads, tail_instances, product_ctas)
+        _check(lib().mayo_b200_shared_set_shape(self.set, ctypes.byref(sh)), "shared_set_shape")
 
     def shared_shape(self) -> dict:
         sh = SharedShape()
         _check(lib().mayo_b200_shared_get_shape(self.set, ctypes.byref(sh)), "shared_get_shape")
-        return {"hash_threads": int(sh.hash_threads), "tail_instances": int(sh.tail_instances)}
+        return {"hash_threads": int(sh.hash_threads), "tail_instances": int(sh.tail_instances),
+                "product_ctas": int(sh.product_ctas)}
 
     @staticmethod
     def shared_timing(enable: bool) -> None:

@@ -7,8 +7,9 @@ later ones fill in as its CTAs finish) — and keeps the fastest.
 
 tune_shared: for one set's sign_shared + verify_shared on a given batch it times the block shapes
 the library can run — threads per CTA of the thread-per-instance hash kernels (32..256) and
-signatures per sign-tail CTA (1, or 2 or 4 with the instances' elimination columns interleaved) — and
-sets the fastest (mayo_b200_shared_set_shape).
+signatures per sign-tail CTA (1, or 2 or 4 with the instances' elimination columns interleaved) and
+CTAs per key-product tile (1, or a CTA pair sharing each tile's key rows) — and sets the fastest
+(mayo_b200_shared_set_shape).
 
 Results are cached per (GPU name, SMs, workload) in a JSON file (MAYO_B200_TUNE_CACHE, default
 ~/.cache/mayo_b200/autotune.json) so later runs skip the search.
@@ -115,7 +116,7 @@ def tune_queue(q: "Q.Queue", items: np.ndarray, repeats: int = 2, use_cache: boo
     return best
 
 
-SHARED_CANDIDATES = [(h, g) for g in (1, 2, 4) for h in (32, 64, 128, 256)]
+SHARED_CANDIDATES = [(h, g, p) for p in (1, 2) for g in (1, 2, 4) for h in (32, 64, 128, 256)]
 
 
 def _lib_id() -> str:
@@ -142,9 +143,9 @@ def tune_shared(m, run, batch: int, repeats: int = 3, flush=None, use_cache: boo
         best = cache[key]
     else:
         trials = []
-        for h, g in SHARED_CANDIDATES:
+        for h, g, p in SHARED_CANDIDATES:
             try:
-                m.set_shared_shape(h, g)
+                m.set_shared_shape(h, g, p)
             except Exception:  # a shape this set's kernels cannot take (shared memory)
                 continue
             run()
@@ -159,10 +160,10 @@ def tune_shared(m, run, batch: int, repeats: int = 3, flush=None, use_cache: boo
                 b.record()
                 torch.cuda.synchronize()
                 ms.append(a.elapsed_time(b))
-            trials.append({"hash_threads": h, "tail_instances": g, "ms": min(ms)})
+            trials.append({"hash_threads": h, "tail_instances": g, "product_ctas": p, "ms": min(ms)})
         best = dict(min(trials, key=lambda t: t["ms"]), trials=trials)
         cache[key] = best
         if use_cache:
             _store(cache)
-    m.set_shared_shape(best["hash_threads"], best["tail_instances"])
+    m.set_shared_shape(best["hash_threads"], best["tail_instances"], best.get("product_ctas", 1))
     return best

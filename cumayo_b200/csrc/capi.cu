@@ -401,15 +401,17 @@ MAYO_B200_API int mayo_b200_sign_shared(int set, const uint8_t *esk, const uint8
 MAYO_B200_API int mayo_b200_shared_timing(int enable) { return kernel_rc(mayo::shared_timing(enable)); }
 
 MAYO_B200_API int mayo_b200_shared_set_shape(int set, const mayo_b200_shared_shape *shape) {
-    return mayo::shared_set_shape(set, shape ? (int)shape->hash_threads : 0, shape ? (int)shape->tail_instances : 0);
+    return mayo::shared_set_shape(set, shape ? (int)shape->hash_threads : 0, shape ? (int)shape->tail_instances : 0,
+                                  shape ? (int)shape->product_ctas : 0);
 }
 
 MAYO_B200_API int mayo_b200_shared_get_shape(int set, mayo_b200_shared_shape *shape) {
     if (!shape) return MAYO_B200_ERR_ARG;
-    int h = 0, g = 0;
-    const int rc = mayo::shared_get_shape(set, &h, &g);
+    int h = 0, g = 0, pc = 0;
+    const int rc = mayo::shared_get_shape(set, &h, &g, &pc);
     shape->hash_threads = (uint32_t)h;
     shape->tail_instances = (uint32_t)g;
+    shape->product_ctas = (uint32_t)pc;
     return rc;
 }
 

@@ -121,6 +121,27 @@ struct SharedProb {
     }
 };
 
+// The same product on a CTA pair (shared_gemm2_kernel, tcgen05 cta_group::2): each MMA has
+// M = 256 vector columns (128 from each CTA) and N = 128 key rows of which each CTA holds 64, so
+// each SM streams half of every key tile.  A tile is stored as two halves, [half][K / 16][64][16]
+// (half 0 = bit planes 0-1, rows 0-63; half 1 = planes 2-3): a CTA's chunk of k-steps is one
+// contiguous run of SLOT2-byte k-steps in its half.
+template <int SET, bool VERIFY>
+struct PairProb {
+    using P = SharedProb<SET, VERIFY>;
+    static constexpr int HROWS = 64;                                  // key rows per CTA and tile
+    static constexpr size_t SLOT2 = (size_t)2 * HROWS * 16;           // one k-step of them
+    static constexpr size_t HALF = P::TILE / 2;                       // bytes of a tile half
+    static constexpr int nch_fit(int ck) {
+        return (int)((SH_SMEM_MAX - (size_t)P::NINST * P::KPAD - P::BAR_BYTES) / (ck * SLOT2));
+    }
+    static constexpr int CK = P::CK_EVEN;
+    static constexpr int NCH = nch_fit(CK) < 16 ? nch_fit(CK) : 16;
+    static_assert(NCH >= 2, "key ring");
+    static_assert((3 * NCH + 7) * 8 + 12 <= (int)P::BAR_BYTES, "barrier area");
+    static constexpr size_t SMEM = (size_t)P::NINST * P::KPAD + (size_t)NCH * CK * SLOT2 + P::BAR_BYTES;
+};
+
 // Workspace: control words ([0] status: 0 = product ran, 1 = it gave up; [1] sign retries), A
 // tiles, (sign) the O planes of the key, per-instance hash results (sign: digest, salt, t, V || r; verify: t), per-instance
 // planes, (sign) the list of instances whose first attempt was singular.
@@ -216,9 +237,9 @@ static const uint32_t *launch_hash_order(const MsgIO &m, uint8_t *ws, size_t bat
 // 32 w + cq(q), cq(q) = 8 ((q >> 2) & 3) + 2 (q & 3) + (q >> 4), the order in which the epilogue's
 // packing of 32 sums lands each coordinate on its bit of a G4 plane) and K bytes 4 c + b'; a
 // tile is G consecutive groups, layout [K / 16][G * 128 rows][16 bytes].  One thread per 16
-// bytes.  Also resets the control words and (sign) writes the key's O planes after the tiles,
-// one thread per item.
-template <int SET, bool VERIFY>
+// bytes (PAIR: the two halves of PairProb).  Also resets the control words and (sign) writes
+// the key's O planes after the tiles, one thread per item.
+template <int SET, bool VERIFY, bool PAIR>
 __global__ void shared_a_kernel(const uint8_t *key, uint8_t *A, uint32_t *ctl, uint4 *opl) {
     using P = SharedProb<SET, VERIFY>;
     using S = Set<SET>;
@@ -252,8 +273,15 @@ __global__ void shared_a_kernel(const uint8_t *key, uint8_t *A, uint32_t *ctl, u
         }
     }
     const int tile = gi / P::G, g = gi - tile * P::G;
-    *reinterpret_cast<uint4 *>(A + (size_t)tile * P::TILE + (size_t)ch * P::KROWS * 16 + (size_t)(g * 128 + rho) * 16) =
-        make_uint4(wd[0], wd[1], wd[2], wd[3]);
+    if constexpr (PAIR) {
+        static_assert(P::G == 1, "pair tiles hold one group");
+        constexpr int H = PairProb<SET, VERIFY>::HROWS;
+        *reinterpret_cast<uint4 *>(A + (size_t)tile * P::TILE + (size_t)(rho / H) * PairProb<SET, VERIFY>::HALF +
+                                   (size_t)ch * H * 16 + (size_t)(rho % H) * 16) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+    } else {
+        *reinterpret_cast<uint4 *>(A + (size_t)tile * P::TILE + (size_t)ch * P::KROWS * 16 +
+                                   (size_t)(g * 128 + rho) * 16) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+    }
 }
 
 // The key tiles hold 0 / 128, so every sum is 128 x (the GF(2) sum): bit 7 of its low byte is the
@@ -535,6 +563,288 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
     }
 }
 
+// ---- the same product on a CTA pair (cluster of two CTAs, tcgen05 cta_group::2) ----
+// Roles as in shared_gemm_kernel, with the key rows of every tile split between the two CTAs:
+//   * each CTA's loader streams its half of the key rows (PairProb layout) into its own ring and
+//     its full[] barrier tracks its own copies;
+//   * in the odd CTA, warp 8 forwards each landed chunk to the even CTA's fwd[] barrier (in chunk
+//     order, so every parity wait is on the current phase);
+//   * the even CTA's issuers wait for both halves (full[], fwd[]) and issue the pair MMAs
+//     (M = 256: 128 vector columns from each CTA; N = 128 key rows, 64 from each CTA); their
+//     commits arrive on both CTAs' empty[] and mma_done[] barriers (multicast to the pair);
+//   * both CTAs' epilogues read their own TMEM (128 vector columns x 128 key rows per M-block),
+//     exactly as in the one-CTA kernel, and hand each accumulator back on the even CTA's
+//     acc_free[] (16 warps).
+// Every wait is bounded; a CTA that gives up sets its failure word, unwinds as the one-CTA
+// kernel does (its own copies, the even CTA's own MMAs), and both CTAs meet at the cluster
+// barrier before TMEM is freed, so no MMA reads a CTA's shared memory after it has left.
+template <int SET, bool VERIFY>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SH_GEMM_NT, 1)
+    shared_gemm2_kernel(const uint8_t *__restrict__ A, const uint8_t *__restrict__ vec, size_t vec_stride,
+                        uint4 *__restrict__ planes, uint32_t batch, uint32_t *ctl, uint32_t spin,
+                        uint32_t stall_after) {
+    using P = SharedProb<SET, VERIFY>;
+    using Q = PairProb<SET, VERIFY>;
+    using S = Set<SET>;
+    constexpr int NIN = P::NINST, KPAD = P::KPAD, NT = P::NTILES, NB = P::NB;
+    constexpr int KR = P::KROWS;
+    constexpr uint32_t NCH = (uint32_t)Q::NCH, CK = (uint32_t)Q::CK, SLOT = (uint32_t)Q::SLOT2;
+    constexpr uint32_t IDESC = tc::idesc_u8(256, KR);
+    constexpr uint32_t ACC = KR * NB;  // TMEM columns of one accumulator
+    static_assert(P::G == 1, "one key group per tile");
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *sB = smem;                                            // [KPAD/16][NIN][16] vector columns
+    uint8_t *ring = smem + (size_t)NIN * KPAD;                      // NCH x CK x [2][64][16] key rows
+    uint64_t *full = reinterpret_cast<uint64_t *>(ring + (size_t)NCH * CK * SLOT);  // [NCH] own copies
+    uint64_t *fwd = full + NCH;                                     // [NCH] even CTA: odd CTA's copies
+    uint64_t *empty = fwd + NCH;                                    // [NCH]
+    uint64_t *mma_done = empty + NCH;                               // [2]
+    uint64_t *acc_free = mma_done + 2;                              // [2] even CTA: 16 epilogue warps
+    uint64_t *drain = acc_free + 2;                                 // [2]
+    uint64_t *vec_ready = drain + 2;                                // even CTA: odd CTA's vectors built
+    uint32_t *s_tmem = reinterpret_cast<uint32_t *>(vec_ready + 1);
+    uint32_t *s_fail = s_tmem + 1;
+    uint32_t *s_loaded = s_tmem + 2;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t rank = tc::cluster_ctarank();
+    const bool lead = rank == 0;
+    const uint32_t inst0 = blockIdx.x * (uint32_t)P::NI;
+
+    if (tid == 0) {
+        for (uint32_t i = 0; i < NCH; i++) {
+            tc::mbar_init(&full[i], 1);
+            tc::mbar_init(&fwd[i], 1);
+            tc::mbar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < 2; i++) {
+            tc::mbar_init(&mma_done[i], 1);
+            tc::mbar_init(&acc_free[i], 2 * SH_EPI_NT / 32);
+        }
+        tc::mbar_init(&drain[0], 1);
+        tc::mbar_init(&drain[1], 1);
+        tc::mbar_init(vec_ready, 1);
+        tc::fence_mbar_init();
+        *s_fail = 0;
+        *s_loaded = 0;
+    }
+    if (warp == 0) {
+        tc::tmem_alloc2(s_tmem, 2 * ACC);
+        tc::tmem_relinquish2();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::cluster_sync();  // both CTAs' barriers and TMEM exist before any arrive or MMA crosses CTAs
+    tc::fence_after_sync();
+    const uint32_t tbase = *s_tmem;
+    auto first_step = [](int tile) { return P::c_min(tile / P::W) / 8; };
+    // both CTAs of a pair walk the tiles in the same order, from the pair's own offset
+    const int t_off = (int)(((blockIdx.x >> 1) % 128u) * (uint32_t)NT / 128u);
+    auto tile_of = [&](int i) { return i + t_off < NT ? i + t_off : i + t_off - NT; };
+    if (warp == SH_LOAD_WARP) {
+        // ---------------- loader (both CTAs): chunk c -> slot c % NCH of this CTA's ring ----------------
+        if (lane == 0) {
+            uint32_t c = 0;
+            bool ok = true, stalled = false;
+#pragma unroll 1
+            for (int i = 0; i < NT && ok && !stalled; i++) {
+                const int t = tile_of(i);
+                const uint8_t *src = A + (size_t)t * P::TILE + (size_t)rank * Q::HALF;
+#pragma unroll 1
+                for (int a = first_step(t); a < P::KSTEPS; a += (int)CK, c++) {
+                    const uint32_t cs = c % NCH;
+                    if (c >= stall_after) {  // failure injection: stop without telling the other warps
+                        stalled = true;
+                        break;
+                    }
+                    if (*reinterpret_cast<volatile uint32_t *>(s_fail) ||
+                        (c >= NCH && !wait_or_fail(&empty[cs], (c / NCH - 1) & 1u, spin, s_fail))) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t n = P::KSTEPS - a < (int)CK ? (uint32_t)(P::KSTEPS - a) : CK;
+                    tc::mbar_arrive_expect_tx(&full[cs], n * SLOT);
+                    tc::bulk_g2s(ring + (size_t)cs * CK * SLOT, src + (size_t)a * SLOT, n * SLOT, &full[cs]);
+                    __threadfence_block();
+                    *reinterpret_cast<volatile uint32_t *>(s_loaded) = c + 1;
+                }
+            }
+            if (!ok) atomicOr(s_fail, 1u);
+            // unwind: no copy of this CTA in flight when it leaves
+            for (uint32_t ch = c > NCH ? c - NCH : 0; ch < c; ch++)
+                tc::mbar_wait(&full[ch % NCH], (ch / NCH) & 1u, SH_SPIN);
+            // and, on a normal end, the even CTA's last commits have arrived on this CTA's empty[]
+            if (ok && !stalled)
+                for (uint32_t ch = c > NCH ? c - NCH : 0; ch < c; ch++)
+                    wait_or_fail(&empty[ch % NCH], (ch / NCH) & 1u, spin, s_fail);
+        }
+    } else {
+        // vector columns, as in shared_gemm_kernel
+        for (int idx = tid; idx < (KPAD / 16) * NIN; idx += SH_LOAD_WARP * 32) {
+            const int ch = idx / NIN, n = idx - ch * NIN;
+            const uint32_t inst = inst0 + (uint32_t)(n / S::k);
+            const int j = n % S::k;
+            uint32_t wd[4] = {0u, 0u, 0u, 0u};
+            if (n < P::NI * S::k && inst < batch && 4 * ch < P::NVEC) {
+                const int nib0 = j * P::NVEC + 4 * ch;
+                const uint32_t x4 = ld_le32(vec + (size_t)inst * vec_stride + (nib0 >> 1)) >> ((nib0 & 1) * 4);
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    if (4 * ch + q < P::NVEC) {
+                        const uint32_t x = (x4 >> (4 * q)) & 0xFu;
+                        wd[q] = (x * 0x00204081u) & 0x01010101u;  // bit b' -> byte b'
+                    }
+                }
+            }
+            *reinterpret_cast<uint4 *>(sB + ((size_t)ch * NIN + n) * 16) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+        }
+        tc::fence_async_smem();
+        bar_sync(1, SH_LOAD_WARP * 32);  // warps 0-9: the vector columns are in place
+        // the even CTA's MMAs read the odd CTA's vector columns too: tell it they are in place
+        if (!lead && tid == 0) tc::mbar_arrive_remote(vec_ready, 0);
+    }
+    if (!lead && warp == SH_ISSUE_WARP) {
+        // ---------------- odd CTA, warp 8: forward each landed chunk to the even CTA ----------------
+        // In chunk order: chunk c - NCH was forwarded before, so slot c % NCH's barrier is in chunk
+        // c's phase and the parity wait cannot pass on an older phase.
+        if (lane == 0) {
+            uint32_t c = 0;
+            bool ok = true;
+#pragma unroll 1
+            for (int i = 0; i < NT && ok; i++) {
+                const int t = tile_of(i);
+#pragma unroll 1
+                for (int a = first_step(t); a < P::KSTEPS; a += (int)CK, c++) {
+                    const uint32_t cs = c % NCH;
+                    if (!wait_or_fail(&full[cs], (c / NCH) & 1u, spin, s_fail)) {
+                        ok = false;
+                        break;
+                    }
+                    tc::mbar_arrive_remote(&fwd[cs], 0);
+                }
+            }
+            if (!ok) atomicOr(s_fail, 1u);
+        }
+    } else if (lead && (warp == SH_ISSUE_WARP || warp == SH_ISSUE_WARP + 1)) {
+        // ---------------- even CTA: MMA issuers, warp 8 the even tiles, warp 9 the odd ones ----------------
+        const int me = warp - SH_ISSUE_WARP;
+        if (lane == 0) {
+            // B: this CTA's half of a k-step, [2][64 rows][16 B] (the odd CTA's half at the same address)
+            const uint64_t kd0 = tc::desc_kmajor(tc::smem_u32(ring), (uint32_t)Q::HROWS * 16u, 128u);
+            const uint64_t vd0 = tc::desc_kmajor(tc::smem_u32(sB), (uint32_t)NIN * 16u, 128u);
+            constexpr uint64_t KD_STEP = SLOT >> 4, VD_STEP = (2u * NIN * 16u) >> 4, VD_BLOCK = 2048u >> 4;
+            uint32_t c = 0;
+            bool ok = tc::mbar_wait_cluster(vec_ready, 0u, spin);  // the odd CTA's vector columns
+#pragma unroll 1
+            for (int i = 0; i < NT && ok; i++) {
+                const int s0 = first_step(tile_of(i));
+                if ((i & 1) != me) {
+                    c += (uint32_t)((P::KSTEPS - s0 + (int)CK - 1) / (int)CK);
+                    continue;
+                }
+                const int b = i & 1;
+                if (i >= 2) {
+                    // both CTAs' epilogues (16 warps, half of them remote) read accumulator b
+                    uint32_t polls = 0;
+                    bool freed = false;
+                    while (polls < spin && !freed) {
+                        freed = tc::mbar_wait_cluster(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, 64);
+                        polls += 64;
+                        if (!freed && *reinterpret_cast<volatile uint32_t *>(s_fail)) break;
+                    }
+                    if (!freed) {
+                        ok = false;
+                        break;
+                    }
+                }
+                tc::fence_after_sync();
+                const uint32_t dacc = tbase + (uint32_t)b * ACC;
+#pragma unroll 1
+                for (int a = s0; a < P::KSTEPS; a += (int)CK, c++) {
+                    const uint32_t cs = c % NCH;
+                    // chunk c armed by this CTA's loader: the slot's barriers are in chunk c's phase
+                    uint32_t polls = 0;
+                    while (*reinterpret_cast<volatile uint32_t *>(s_loaded) <= c && ++polls < spin) {
+                    }
+                    __threadfence_block();
+                    if (polls >= spin || !tc::mbar_wait(&full[cs], (c / NCH) & 1u, spin) ||
+                        !tc::mbar_wait_cluster(&fwd[cs], (c / NCH) & 1u, spin)) {
+                        ok = false;
+                        break;
+                    }
+                    const int n = P::KSTEPS - a;
+                    const uint64_t kdc = kd0 + (uint64_t)cs * (CK * KD_STEP);
+                    const uint64_t vdc = vd0 + (uint64_t)a * VD_STEP;
+                    const uint32_t acc0 = a > s0 ? 1u : 0u;
+#pragma unroll
+                    for (int u = 0; u < (int)CK; u++) {
+                        if (u < n) {
+#pragma unroll
+                            for (int h = 0; h < NB; h++)
+                                tc::mma2_i8(dacc + (uint32_t)h * KR, vdc + (uint64_t)u * VD_STEP + (uint64_t)h * VD_BLOCK,
+                                            kdc + (uint64_t)u * KD_STEP, IDESC, u > 0 ? 1u : acc0);
+                        }
+                    }
+                    tc::mma2_commit_mc(&empty[cs], 0x3);  // both CTAs may refill the chunk's slot
+                }
+                if (!ok) break;
+                tc::mma2_commit_mc(&mma_done[b], 0x3);  // both CTAs' epilogues may read accumulator b
+                if ((i & 15) == me && *reinterpret_cast<volatile uint32_t *>(s_fail)) ok = false;
+            }
+            if (!ok) atomicOr(s_fail, 1u);
+            // unwind: every MMA this thread issued (reading both CTAs' shared memory) has completed
+            tc::mma2_commit_mc(&drain[me], 0x1);
+            tc::mbar_wait(&drain[me], 0u, SH_SPIN);
+        }
+    } else if (warp < SH_ISSUE_WARP) {
+        // ---------------- epilogue (both CTAs), as in shared_gemm_kernel ----------------
+        constexpr int PL = 4;
+        static_assert(NB == 2, "two M-blocks: warps 0-3 block 0, warps 4-7 block 1");
+        const int grp = warp & 3, h = warp >> 2;
+        const int n = h * 128 + grp * 32 + lane;
+        const uint32_t inst = inst0 + (uint32_t)(n / S::k);
+        const int j = n % S::k;
+        const bool live = n < P::NI * S::k && inst < batch;
+        uint4 *dst = planes + (size_t)inst * P::PLANES + (size_t)j * P::NROWS * P::W;
+        const uint32_t taddr = tbase + ((uint32_t)(grp * 32) << 16) + (uint32_t)(h * KR);
+#pragma unroll 1
+        for (int i = 0; i < NT; i++) {
+            const int b = i & 1;
+            if (!wait_or_fail(&mma_done[b], (uint32_t)(i >> 1) & 1u, spin, s_fail)) {
+                atomicOr(s_fail, 1u);
+                break;
+            }
+            tc::fence_after_sync();
+            uint32_t r[PL][16];
+#pragma unroll
+            for (int p = 0; p < PL; p++) tc::tmem_ld32_pack16(taddr + (uint32_t)b * ACC + (uint32_t)p * 32u, r[p]);
+            tc::tmem_wait_ld();
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) {  // accumulator b may be overwritten now (as far as this warp goes)
+                if (lead) tc::mbar_arrive(&acc_free[b]);
+                else tc::mbar_arrive_remote(&acc_free[b], 0);
+            }
+            uint32_t wd[PL];
+#pragma unroll
+            for (int p = 0; p < PL; p++) wd[p] = pack_bit7x32(r[p]);
+            const int gi = tile_of(i);
+            if (live && gi < P::NGROUPS)
+                *reinterpret_cast<uint4 *>(dst + gi) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+            if (*reinterpret_cast<volatile uint32_t *>(s_fail)) break;
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    // the pair meets here: the even CTA's MMAs and every arrive that crosses CTAs are complete,
+    // so neither CTA's shared memory is read or written after it leaves
+    tc::cluster_sync();
+    if (tid == 0 && *s_fail) atomicOr(ctl, 1u);
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc2(tbase, 2 * ACC);
+    }
+}
+
 // ---- sign ----
 // First attempt from the planes, in a CTA without engine staging (more CTAs per SM).  A singular
 // first attempt goes to the retry list; the fix-up kernel finishes it with the engine.
@@ -743,6 +1053,7 @@ static void tmark(cudaStream_t st) {
 struct SharedShape {
     std::atomic<int> hash_nt{HASH_NT};  // threads per CTA of the thread-per-instance hash kernels
     std::atomic<int> tail_g{1};         // instances per sign-tail CTA
+    std::atomic<int> pair{0};           // the key product on CTA pairs (shared_gemm2_kernel)
 };
 SharedShape g_shape[4];
 static int shape_index(int set) { return set == 1 ? 0 : set == 2 ? 1 : set == 3 ? 2 : set == 5 ? 3 : -1; }
@@ -755,17 +1066,31 @@ static int launch_product(const uint8_t *key, const uint8_t *vec, size_t vec_str
     using WSL = SharedWs<SET, VERIFY>;
     uint32_t *ctl = reinterpret_cast<uint32_t *>(ws);
     uint8_t *A = ws + WSL::a;
+    const bool pair = g_shape[shape_index(SET)].pair.load(std::memory_order_relaxed) != 0;
     const size_t a_threads = (size_t)P::NTILES * P::G * (P::KPAD / 16) * 128 + WSL::OPL;
-    shared_a_kernel<SET, VERIFY><<<(unsigned)((a_threads + 255) / 256), 256, 0, st>>>(
-        key, A, ctl, reinterpret_cast<uint4 *>(ws + WSL::op_off()));
+    if (pair)
+        shared_a_kernel<SET, VERIFY, true><<<(unsigned)((a_threads + 255) / 256), 256, 0, st>>>(
+            key, A, ctl, reinterpret_cast<uint4 *>(ws + WSL::op_off()));
+    else
+        shared_a_kernel<SET, VERIFY, false><<<(unsigned)((a_threads + 255) / 256), 256, 0, st>>>(
+            key, A, ctl, reinterpret_cast<uint4 *>(ws + WSL::op_off()));
     tmark(st);
-    if (!set_smem_attr(shared_gemm_kernel<SET, VERIFY>, P::SMEM)) return ST_CUDA;
     uint4 *planes = reinterpret_cast<uint4 *>(ws + WSL::planes_off(batch));
     const Inject &inj = inject();
     const bool stall = inj.kind == MAYO_B200_INJECT_PRODUCT_STALL;
     const uint32_t spin = stall && inj.spin ? inj.spin : SH_SPIN;
-    shared_gemm_kernel<SET, VERIFY><<<(unsigned)((batch + P::NI - 1) / P::NI), SH_GEMM_NT, P::SMEM, st>>>(
-        A, vec, vec_stride, planes, (uint32_t)batch, ctl, spin, stall ? inj.arg : 0xFFFFFFFFu);
+    const unsigned ctas = (unsigned)((batch + P::NI - 1) / P::NI);
+    if (pair) {
+        using Q = PairProb<SET, VERIFY>;
+        if (!set_smem_attr(shared_gemm2_kernel<SET, VERIFY>, Q::SMEM)) return ST_CUDA;
+        // clusters of two: an even number of CTAs (a last CTA without instances still takes part)
+        shared_gemm2_kernel<SET, VERIFY><<<(ctas + 1) / 2 * 2, SH_GEMM_NT, Q::SMEM, st>>>(
+            A, vec, vec_stride, planes, (uint32_t)batch, ctl, spin, stall ? inj.arg : 0xFFFFFFFFu);
+    } else {
+        if (!set_smem_attr(shared_gemm_kernel<SET, VERIFY>, P::SMEM)) return ST_CUDA;
+        shared_gemm_kernel<SET, VERIFY><<<ctas, SH_GEMM_NT, P::SMEM, st>>>(
+            A, vec, vec_stride, planes, (uint32_t)batch, ctl, spin, stall ? inj.arg : 0xFFFFFFFFu);
+    }
     tmark(st);
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
 }
@@ -890,23 +1215,27 @@ static size_t tail_smem(int set, int g) {
     }
 }
 
-int shared_set_shape(int set, int hash_nt, int tail_g) {
+int shared_set_shape(int set, int hash_nt, int tail_g, int product_ctas) {
     const int si = shape_index(set);
     if (si < 0) return ST_BAD_SET;
     if (hash_nt == 0) hash_nt = HASH_NT;
     if (tail_g == 0) tail_g = 1;
     if (hash_nt < 32 || hash_nt > 1024 || hash_nt % 32 || (tail_g != 1 && tail_g != 2 && tail_g != 4)) return ST_BAD_ARG;
     if (tail_smem(set, tail_g) > SH_SMEM_MAX) return ST_BAD_ARG;
+    if (product_ctas == 0) product_ctas = 1;
+    if (product_ctas != 1 && product_ctas != 2) return ST_BAD_ARG;
     g_shape[si].hash_nt.store(hash_nt);
     g_shape[si].tail_g.store(tail_g);
+    g_shape[si].pair.store(product_ctas == 2 ? 1 : 0);
     return ST_OK;
 }
 
-int shared_get_shape(int set, int *hash_nt, int *tail_g) {
+int shared_get_shape(int set, int *hash_nt, int *tail_g, int *product_ctas) {
     const int si = shape_index(set);
     if (si < 0) return ST_BAD_SET;
     *hash_nt = g_shape[si].hash_nt.load();
     *tail_g = g_shape[si].tail_g.load();
+    *product_ctas = g_shape[si].pair.load() ? 2 : 1;
     return ST_OK;
 }
 

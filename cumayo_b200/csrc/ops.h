@@ -84,9 +84,10 @@ int launch_sign_shared(int set, const SignIO &io, uint8_t *ws, size_t batch, cud
 int launch_verify_shared(int set, const VerifyIO &io, uint8_t *ws, size_t batch, cudaStream_t st);
 int shared_timing(int enable);
 int shared_timing_read(float *ms);
-// Runtime shape of the shared-key path per set: hash-kernel CTA threads, sign-tail instances per CTA.
-int shared_set_shape(int set, int hash_nt, int tail_g);
-int shared_get_shape(int set, int *hash_nt, int *tail_g);
+// Runtime shape of the shared-key path per set: hash-kernel CTA threads, sign-tail instances per
+// CTA, CTAs per key-product tile (1, or a CTA pair).
+int shared_set_shape(int set, int hash_nt, int tail_g, int product_ctas);
+int shared_get_shape(int set, int *hash_nt, int *tail_g, int *product_ctas);
 
 // Status plumbing of the C-ABI (capi.cu): a failed CUDA call or launch is recorded as the calling
 // thread's last CUDA error (mayo_b200_last_cuda_error) and reported as ST_CUDA.  api_launch_rc

@@ -123,8 +123,9 @@ def test_shared_key_large_batch(cuda, s):
 
 @pytest.mark.parametrize("s", [1, 2, 3, 5])
 def test_shared_key_block_shapes(cuda, s):
-    """Every block shape the autotuner may choose (hash CTA threads, sign-tail instances per CTA)
-    gives the bytes of the per-instance path, also for an odd batch (a last CTA half empty)."""
+    """Every block shape the autotuner may choose (hash CTA threads, sign-tail instances per CTA,
+    CTAs per key-product tile) gives the bytes of the per-instance path, also for an odd batch
+    (a last CTA half empty; with CTA pairs, an odd number of product CTAs)."""
     import torch
     m = Mayo(s)
     z = m.sizes
@@ -144,19 +145,20 @@ def test_shared_key_block_shapes(cuda, s):
     m.verify_many(epk, d_msg, sig_ref, res_ref, n, msg_off=d_off, msg_len=d_len)
     ws = torch.zeros(max(m.sign_shared_ws_bytes(n), m.verify_shared_ws_bytes(n)), dtype=torch.uint8, device="cuda")
     try:
-        for h, g in ((32, 2), (128, 4), (256, 1), (64, 1)):
+        for h, g, p in ((32, 2, 1), (128, 4, 1), (256, 1, 1), (64, 1, 2), (64, 4, 2)):
             try:
-                m.set_shared_shape(h, g)
+                m.set_shared_shape(h, g, p)
             except MayoError:  # four MAYO_5 tails do not fit in one CTA's shared memory
                 assert s == 5 and g == 4
                 continue
-            assert m.shared_shape() == {"hash_threads": h, "tail_instances": g}
+            assert m.shared_shape() == {"hash_threads": h, "tail_instances": g, "product_ctas": p}
             sig = torch.zeros_like(sig_ref)
             m.sign_shared(esk, d_msg, sig, ws, n, msg_off=d_off, msg_len=d_len)
             res = torch.full((n,), 0xEE, dtype=torch.uint8, device="cuda")
             m.verify_shared(epk, d_msg, sig, res, ws, n, msg_off=d_off, msg_len=d_len)
             torch.cuda.synchronize()
-            assert torch.equal(sig, sig_ref), (h, g)
-            assert torch.equal(res, res_ref) and int(res.sum()) == 0, (h, g)
+            assert int(ws[:4].cpu().numpy().view(np.uint32)[0]) == 0, ("product gave up", h, g, p)
+            assert torch.equal(sig, sig_ref), (h, g, p)
+            assert torch.equal(res, res_ref) and int(res.sum()) == 0, (h, g, p)
     finally:
-        m.set_shared_shape(0, 0)
+        m.set_shared_shape(0, 0, 0)
