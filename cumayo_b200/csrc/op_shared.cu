@@ -306,6 +306,33 @@ __device__ __forceinline__ bool wait_or_fail(uint64_t *bar, uint32_t parity, uin
     return false;
 }
 
+// Whole-warp forms for the MMA issuers, whose loop every lane runs so that the values the MMAs
+// take stay warp-uniform; each result is the same in every lane.
+constexpr uint32_t WARP_ALL = 0xFFFFFFFFu;
+__device__ __forceinline__ bool warp_wait_or_fail(uint64_t *bar, uint32_t parity, uint32_t limit, const uint32_t *fail) {
+    return __all_sync(WARP_ALL, wait_or_fail(bar, parity, limit, fail));
+}
+// The same for an mbarrier that the other CTA of a pair arrives on (acquire at cluster scope).
+__device__ __forceinline__ bool warp_wait_cluster_or_fail(uint64_t *bar, uint32_t parity, uint32_t limit,
+                                                          const uint32_t *fail) {
+    bool seen = false;
+    for (uint32_t i = 0; i < limit && !seen; i += 64) {
+        seen = tc::mbar_wait_cluster(bar, parity, 64);
+        if (!seen && *reinterpret_cast<const volatile uint32_t *>(fail)) break;
+    }
+    return __all_sync(WARP_ALL, seen);
+}
+__device__ __forceinline__ bool warp_flag(const uint32_t *f) {
+    return __any_sync(WARP_ALL, *reinterpret_cast<const volatile uint32_t *>(f) != 0);
+}
+// Bounded wait until the loader has started chunk c's copy (armed the slot's barrier for it).
+__device__ __forceinline__ bool warp_wait_armed(const uint32_t *loaded, uint32_t c, uint32_t limit) {
+    for (uint32_t polls = 0; __any_sync(WARP_ALL, *reinterpret_cast<const volatile uint32_t *>(loaded) <= c);)
+        if (++polls >= limit) return false;
+    __threadfence_block();
+    return true;
+}
+
 // vec: instance i's vectors start at vec + i * vec_stride, entry c of vector j is nibble
 // j * NVEC + c.  planes: instance i at planes + i * PLANES, [j][row][w].
 //
@@ -444,49 +471,50 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
     }
     if (warp == SH_ISSUE_WARP || warp == SH_ISSUE_WARP + 1) {
         // ---------------- MMA issuers: warp 8 the even tiles, warp 9 the odd ones ----------------
-        // Two issuers, so one issues while the other waits and does its bookkeeping: tiles are
-        // only 5-20 k-steps, and a single thread's per-tile overhead left the tensor pipe idle.
+        // Two issuers, so one issues while the other waits and does its bookkeeping (tiles are
+        // only 1-20 k-steps).  The whole warp runs the loop and the waits, so every value the
+        // MMAs take is warp-uniform; one lane (the same throughout: a commit tracks the MMAs of
+        // the thread that issues it) issues the MMAs and commits.  Run by one lane alone, every
+        // step of this loop took 100-300 cycles and the tensor pipe waited for the issuers.
         const int me = warp - SH_ISSUE_WARP;
-        if (lane == 0) {
-            const uint64_t kd0 = tc::desc_kmajor(tc::smem_u32(ring), (uint32_t)KR * 16u, 128u);
-            const uint64_t vd0 = tc::desc_kmajor(tc::smem_u32(sB), (uint32_t)NIN * 16u, 128u);
-            // descriptor start addresses are in 16-byte units (bits 0-13; every address here is
-            // below 2^18 bytes, so adding to the descriptor never carries out of the field)
-            constexpr uint64_t KD_STEP = SLOT >> 4, VD_STEP = (2u * NIN * 16u) >> 4, VD_BLOCK = 2048u >> 4;
-            uint32_t c = 0;  // global chunk number (the loader's order)
-            bool ok = true;
+        const bool leader = tc::elect_one();
+        const uint64_t kd0 = tc::desc_kmajor(tc::smem_u32(ring), (uint32_t)KR * 16u, 128u);
+        const uint64_t vd0 = tc::desc_kmajor(tc::smem_u32(sB), (uint32_t)NIN * 16u, 128u);
+        // descriptor start addresses are in 16-byte units (bits 0-13; every address here is
+        // below 2^18 bytes, so adding to the descriptor never carries out of the field)
+        constexpr uint64_t KD_STEP = SLOT >> 4, VD_STEP = (2u * NIN * 16u) >> 4, VD_BLOCK = 2048u >> 4;
+        uint32_t c = 0;  // global chunk number (the loader's order)
+        bool ok = true;
 #pragma unroll 1
-            for (int i = 0; i < NT && ok; i++) {
-                const int s0 = first_step(tile_of(i));
-                if ((i & 1) != me) {  // the other issuer's tile: skip its chunks
-                    c += (uint32_t)((P::KSTEPS - s0 + (int)CK - 1) / (int)CK);
-                    continue;
-                }
-                const int b = i & 1;
-                if (i >= 2 && !wait_or_fail(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, spin, s_fail)) {
+        for (int i = 0; i < NT && ok; i++) {
+            const int s0 = first_step(tile_of(i));
+            if ((i & 1) != me) {  // the other issuer's tile: skip its chunks
+                c += (uint32_t)((P::KSTEPS - s0 + (int)CK - 1) / (int)CK);
+                continue;
+            }
+            const int b = i & 1;
+            if (i >= 2 && !warp_wait_or_fail(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, spin, s_fail)) {
+                ok = false;
+                break;
+            }
+            tc::fence_after_sync();
+            const uint32_t dacc = tbase + (uint32_t)b * ACC;
+#pragma unroll 1
+            for (int a = s0; a < P::KSTEPS; a += (int)CK, c++) {
+                const uint32_t cs = c % NCH;
+                // The other issuer's tile may hold unloaded chunks older than c, so slot cs can
+                // still be a phase behind chunk c: a parity wait is only meaningful once the
+                // loader has armed chunk c's phase.
+                if (!warp_wait_armed(s_loaded, c, spin) ||
+                    !__all_sync(WARP_ALL, tc::mbar_wait(&full[cs], (c / NCH) & 1u, spin))) {
                     ok = false;
                     break;
                 }
-                tc::fence_after_sync();
-                const uint32_t dacc = tbase + (uint32_t)b * ACC;
-#pragma unroll 1
-                for (int a = s0; a < P::KSTEPS; a += (int)CK, c++) {
-                    const uint32_t cs = c % NCH;
-                    // The other issuer's tile may hold unloaded chunks older than c, so slot cs
-                    // can still be a phase behind chunk c: a parity wait is only meaningful once
-                    // the loader has armed chunk c's phase.
-                    uint32_t polls = 0;
-                    while (*reinterpret_cast<volatile uint32_t *>(s_loaded) <= c && ++polls < spin) {
-                    }
-                    __threadfence_block();
-                    if (polls >= spin || !tc::mbar_wait(&full[cs], (c / NCH) & 1u, spin)) {
-                        ok = false;
-                        break;
-                    }
-                    const int n = P::KSTEPS - a;  // k-steps of this chunk: min(n, CK)
-                    const uint64_t kdc = kd0 + (uint64_t)cs * (CK * KD_STEP);
-                    const uint64_t vdc = vd0 + (uint64_t)a * VD_STEP;
-                    const uint32_t acc0 = a > s0 ? 1u : 0u;
+                const int n = P::KSTEPS - a;  // k-steps of this chunk: min(n, CK)
+                const uint64_t kdc = kd0 + (uint64_t)cs * (CK * KD_STEP);
+                const uint64_t vdc = vd0 + (uint64_t)a * VD_STEP;
+                const uint32_t acc0 = a > s0 ? 1u : 0u;
+                if (leader) {
 #pragma unroll
                     for (int u = 0; u < (int)CK; u++) {
                         if (u < n) {
@@ -498,16 +526,19 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
                     }
                     tc::mma_commit(&empty[cs]);  // the chunk may be refilled once these MMAs completed
                 }
-                if (!ok) break;
-                tc::mma_commit(&mma_done[b]);  // the accumulator may be read
-                if ((i & 15) == me && *reinterpret_cast<volatile uint32_t *>(s_fail)) ok = false;
+                __syncwarp();
             }
-            if (!ok) atomicOr(s_fail, 1u);
-            // unwind: every MMA of this thread (and so every commit arrival it issued before)
-            // lands before TMEM is freed
-            tc::mma_commit(&drain[me]);
-            tc::mbar_wait(&drain[me], 0u, SH_SPIN);
+            if (!ok) break;
+            if (leader) tc::mma_commit(&mma_done[b]);  // the accumulator may be read
+            __syncwarp();
+            if ((i & 15) == me && warp_flag(s_fail)) ok = false;
         }
+        if (!ok && leader) atomicOr(s_fail, 1u);
+        // unwind: every MMA of this warp (and so every commit arrival it issued before) lands
+        // before TMEM is freed
+        if (leader) tc::mma_commit(&drain[me]);
+        __syncwarp();
+        tc::mbar_wait(&drain[me], 0u, SH_SPIN);
     } else if (warp < SH_ISSUE_WARP) {
         // ---------------- epilogue ----------------
         // warp: TMEM lanes 32 (warp % 4).. = vector columns.  Warps 0-3 / 4-7 split the work:
@@ -705,76 +736,67 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SH_GEMM_NT, 1)
     if (!lead && warp == SH_ISSUE_WARP) {
         // ---------------- odd CTA, warp 8: forward each landed chunk to the even CTA ----------------
         // In chunk order: chunk c - NCH was forwarded before, so slot c % NCH's barrier is in chunk
-        // c's phase and the parity wait cannot pass on an older phase.
-        if (lane == 0) {
-            uint32_t c = 0;
-            bool ok = true;
+        // c's phase and the parity wait cannot pass on an older phase.  The whole warp waits (as
+        // the issuers do); one lane arrives.
+        const bool leader = tc::elect_one();
+        uint32_t c = 0;
+        bool ok = true;
 #pragma unroll 1
-            for (int i = 0; i < NT && ok; i++) {
-                const int t = tile_of(i);
+        for (int i = 0; i < NT && ok; i++) {
+            const int t = tile_of(i);
 #pragma unroll 1
-                for (int a = first_step(t); a < P::KSTEPS; a += (int)CK, c++) {
-                    const uint32_t cs = c % NCH;
-                    if (!wait_or_fail(&full[cs], (c / NCH) & 1u, spin, s_fail)) {
-                        ok = false;
-                        break;
-                    }
-                    tc::mbar_arrive_remote(&fwd[cs], 0);
+            for (int a = first_step(t); a < P::KSTEPS; a += (int)CK, c++) {
+                const uint32_t cs = c % NCH;
+                if (!warp_wait_or_fail(&full[cs], (c / NCH) & 1u, spin, s_fail)) {
+                    ok = false;
+                    break;
                 }
+                if (leader) tc::mbar_arrive_remote_relaxed(&fwd[cs], 0);  // the chunk's bytes have landed
+                __syncwarp();
             }
-            if (!ok) atomicOr(s_fail, 1u);
         }
+        if (!ok && leader) atomicOr(s_fail, 1u);
     } else if (lead && (warp == SH_ISSUE_WARP || warp == SH_ISSUE_WARP + 1)) {
         // ---------------- even CTA: MMA issuers, warp 8 the even tiles, warp 9 the odd ones ----------------
+        // As in shared_gemm_kernel: the whole warp runs the loop, one lane issues and commits.
         const int me = warp - SH_ISSUE_WARP;
-        if (lane == 0) {
-            // B: this CTA's half of a k-step, [2][64 rows][16 B] (the odd CTA's half at the same address)
-            const uint64_t kd0 = tc::desc_kmajor(tc::smem_u32(ring), (uint32_t)Q::HROWS * 16u, 128u);
-            const uint64_t vd0 = tc::desc_kmajor(tc::smem_u32(sB), (uint32_t)NIN * 16u, 128u);
-            constexpr uint64_t KD_STEP = SLOT >> 4, VD_STEP = (2u * NIN * 16u) >> 4, VD_BLOCK = 2048u >> 4;
-            uint32_t c = 0;
-            bool ok = tc::mbar_wait_cluster(vec_ready, 0u, spin);  // the odd CTA's vector columns
+        const bool leader = tc::elect_one();
+        // B: this CTA's half of a k-step, [2][64 rows][16 B] (the odd CTA's half at the same address)
+        const uint64_t kd0 = tc::desc_kmajor(tc::smem_u32(ring), (uint32_t)Q::HROWS * 16u, 128u);
+        const uint64_t vd0 = tc::desc_kmajor(tc::smem_u32(sB), (uint32_t)NIN * 16u, 128u);
+        constexpr uint64_t KD_STEP = SLOT >> 4, VD_STEP = (2u * NIN * 16u) >> 4, VD_BLOCK = 2048u >> 4;
+        uint32_t c = 0;
+        bool ok = warp_wait_cluster_or_fail(vec_ready, 0u, spin, s_fail);  // the odd CTA's vector columns
 #pragma unroll 1
-            for (int i = 0; i < NT && ok; i++) {
-                const int s0 = first_step(tile_of(i));
-                if ((i & 1) != me) {
-                    c += (uint32_t)((P::KSTEPS - s0 + (int)CK - 1) / (int)CK);
-                    continue;
-                }
-                const int b = i & 1;
-                if (i >= 2) {
-                    // both CTAs' epilogues (16 warps, half of them remote) read accumulator b
-                    uint32_t polls = 0;
-                    bool freed = false;
-                    while (polls < spin && !freed) {
-                        freed = tc::mbar_wait_cluster(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, 64);
-                        polls += 64;
-                        if (!freed && *reinterpret_cast<volatile uint32_t *>(s_fail)) break;
-                    }
-                    if (!freed) {
-                        ok = false;
-                        break;
-                    }
-                }
-                tc::fence_after_sync();
-                const uint32_t dacc = tbase + (uint32_t)b * ACC;
+        for (int i = 0; i < NT && ok; i++) {
+            const int s0 = first_step(tile_of(i));
+            if ((i & 1) != me) {
+                c += (uint32_t)((P::KSTEPS - s0 + (int)CK - 1) / (int)CK);
+                continue;
+            }
+            const int b = i & 1;
+            // both CTAs' epilogues (16 warps, half of them remote) read accumulator b
+            if (i >= 2 && !warp_wait_cluster_or_fail(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, spin, s_fail)) {
+                ok = false;
+                break;
+            }
+            tc::fence_after_sync();
+            const uint32_t dacc = tbase + (uint32_t)b * ACC;
 #pragma unroll 1
-                for (int a = s0; a < P::KSTEPS; a += (int)CK, c++) {
-                    const uint32_t cs = c % NCH;
-                    // chunk c armed by this CTA's loader: the slot's barriers are in chunk c's phase
-                    uint32_t polls = 0;
-                    while (*reinterpret_cast<volatile uint32_t *>(s_loaded) <= c && ++polls < spin) {
-                    }
-                    __threadfence_block();
-                    if (polls >= spin || !tc::mbar_wait(&full[cs], (c / NCH) & 1u, spin) ||
-                        !tc::mbar_wait_cluster(&fwd[cs], (c / NCH) & 1u, spin)) {
-                        ok = false;
-                        break;
-                    }
-                    const int n = P::KSTEPS - a;
-                    const uint64_t kdc = kd0 + (uint64_t)cs * (CK * KD_STEP);
-                    const uint64_t vdc = vd0 + (uint64_t)a * VD_STEP;
-                    const uint32_t acc0 = a > s0 ? 1u : 0u;
+            for (int a = s0; a < P::KSTEPS; a += (int)CK, c++) {
+                const uint32_t cs = c % NCH;
+                // chunk c armed by this CTA's loader: the slot's barriers are in chunk c's phase
+                if (!warp_wait_armed(s_loaded, c, spin) ||
+                    !__all_sync(WARP_ALL, tc::mbar_wait(&full[cs], (c / NCH) & 1u, spin)) ||
+                    !__all_sync(WARP_ALL, tc::mbar_wait_cluster(&fwd[cs], (c / NCH) & 1u, spin))) {
+                    ok = false;
+                    break;
+                }
+                const int n = P::KSTEPS - a;
+                const uint64_t kdc = kd0 + (uint64_t)cs * (CK * KD_STEP);
+                const uint64_t vdc = vd0 + (uint64_t)a * VD_STEP;
+                const uint32_t acc0 = a > s0 ? 1u : 0u;
+                if (leader) {
 #pragma unroll
                     for (int u = 0; u < (int)CK; u++) {
                         if (u < n) {
@@ -786,15 +808,18 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SH_GEMM_NT, 1)
                     }
                     tc::mma2_commit_mc(&empty[cs], 0x3);  // both CTAs may refill the chunk's slot
                 }
-                if (!ok) break;
-                tc::mma2_commit_mc(&mma_done[b], 0x3);  // both CTAs' epilogues may read accumulator b
-                if ((i & 15) == me && *reinterpret_cast<volatile uint32_t *>(s_fail)) ok = false;
+                __syncwarp();
             }
-            if (!ok) atomicOr(s_fail, 1u);
-            // unwind: every MMA this thread issued (reading both CTAs' shared memory) has completed
-            tc::mma2_commit_mc(&drain[me], 0x1);
-            tc::mbar_wait(&drain[me], 0u, SH_SPIN);
+            if (!ok) break;
+            if (leader) tc::mma2_commit_mc(&mma_done[b], 0x3);  // both CTAs' epilogues may read accumulator b
+            __syncwarp();
+            if ((i & 15) == me && warp_flag(s_fail)) ok = false;
         }
+        if (!ok && leader) atomicOr(s_fail, 1u);
+        // unwind: every MMA this warp issued (reading both CTAs' shared memory) has completed
+        if (leader) tc::mma2_commit_mc(&drain[me], 0x1);
+        __syncwarp();
+        tc::mbar_wait(&drain[me], 0u, SH_SPIN);
     } else if (warp < SH_ISSUE_WARP) {
         // ---------------- epilogue (both CTAs), as in shared_gemm_kernel ----------------
         constexpr int PL = 4;
@@ -821,8 +846,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SH_GEMM_NT, 1)
             tc::fence_before_sync();
             __syncwarp();
             if (lane == 0) {  // accumulator b may be overwritten now (as far as this warp goes)
+                // relaxed: the loads above have completed (wait::ld), and a release would first
+                // wait for this warp's plane stores of the previous tile
                 if (lead) tc::mbar_arrive(&acc_free[b]);
-                else tc::mbar_arrive_remote(&acc_free[b], 0);
+                else tc::mbar_arrive_remote_relaxed(&acc_free[b], 0);
             }
             uint32_t wd[PL];
 #pragma unroll
