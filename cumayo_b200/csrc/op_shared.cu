@@ -493,11 +493,6 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
                 continue;
             }
             const int b = i & 1;
-            if (i >= 2 && !warp_wait_or_fail(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, spin, s_fail)) {
-                ok = false;
-                break;
-            }
-            tc::fence_after_sync();
             const uint32_t dacc = tbase + (uint32_t)b * ACC;
 #pragma unroll 1
             for (int a = s0; a < P::KSTEPS; a += (int)CK, c++) {
@@ -509,6 +504,16 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
                     !__all_sync(WARP_ALL, tc::mbar_wait(&full[cs], (c / NCH) & 1u, spin))) {
                     ok = false;
                     break;
+                }
+                // Only now wait for accumulator b (the epilogue of tile i - 2): the checks above
+                // and the loop's bookkeeping then overlap that epilogue, and the MMAs follow the
+                // accumulator's release at once.
+                if (a == s0) {
+                    if (i >= 2 && !warp_wait_or_fail(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, spin, s_fail)) {
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_after_sync();
                 }
                 const int n = P::KSTEPS - a;  // k-steps of this chunk: min(n, CK)
                 const uint64_t kdc = kd0 + (uint64_t)cs * (CK * KD_STEP);
@@ -775,12 +780,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SH_GEMM_NT, 1)
                 continue;
             }
             const int b = i & 1;
-            // both CTAs' epilogues (16 warps, half of them remote) read accumulator b
-            if (i >= 2 && !warp_wait_cluster_or_fail(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, spin, s_fail)) {
-                ok = false;
-                break;
-            }
-            tc::fence_after_sync();
             const uint32_t dacc = tbase + (uint32_t)b * ACC;
 #pragma unroll 1
             for (int a = s0; a < P::KSTEPS; a += (int)CK, c++) {
@@ -791,6 +790,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SH_GEMM_NT, 1)
                     !__all_sync(WARP_ALL, tc::mbar_wait_cluster(&fwd[cs], (c / NCH) & 1u, spin))) {
                     ok = false;
                     break;
+                }
+                // then accumulator b: both CTAs' epilogues (16 warps, half of them remote) have
+                // read tile i - 2 from it
+                if (a == s0) {
+                    if (i >= 2 && !warp_wait_cluster_or_fail(&acc_free[b], (uint32_t)((i - 2) >> 1) & 1u, spin, s_fail)) {
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_after_sync();
                 }
                 const int n = P::KSTEPS - a;
                 const uint64_t kdc = kd0 + (uint64_t)cs * (CK * KD_STEP);
@@ -1078,11 +1086,16 @@ static void tmark(cudaStream_t st) {
 
 // ---- runtime shape of the shared-key path, per parameter set (mayo_b200_shared_set_shape) ----
 struct SharedShape {
-    std::atomic<int> hash_nt{HASH_NT};  // threads per CTA of the thread-per-instance hash kernels
-    std::atomic<int> tail_g{1};         // instances per sign-tail CTA
-    std::atomic<int> pair{0};           // the key product on CTA pairs (shared_gemm2_kernel)
+    std::atomic<int> hash_nt;  // threads per CTA of the thread-per-instance hash kernels
+    std::atomic<int> tail_g;   // instances per sign-tail CTA
+    std::atomic<int> pair;     // the key product on CTA pairs (shared_gemm2_kernel)
 };
-SharedShape g_shape[4];
+// Defaults (MAYO_1, 2, 3, 5), measured at 65,536 instances: the pair product is the faster one
+// for every set (MAYO_5 sign 14.0 against 18.5 ms: one CTA's key ring holds only four chunks
+// beside its vectors), and four signatures per sign-tail CTA pay only for MAYO_2.
+constexpr int default_tail_g(int si) { return si == 1 ? 4 : 1; }
+SharedShape g_shape[4] = {{HASH_NT, default_tail_g(0), 1}, {HASH_NT, default_tail_g(1), 1},
+                          {HASH_NT, default_tail_g(2), 1}, {HASH_NT, default_tail_g(3), 1}};
 static int shape_index(int set) { return set == 1 ? 0 : set == 2 ? 1 : set == 3 ? 2 : set == 5 ? 3 : -1; }
 
 // ---- launchers ----
@@ -1246,10 +1259,10 @@ int shared_set_shape(int set, int hash_nt, int tail_g, int product_ctas) {
     const int si = shape_index(set);
     if (si < 0) return ST_BAD_SET;
     if (hash_nt == 0) hash_nt = HASH_NT;
-    if (tail_g == 0) tail_g = 1;
+    if (tail_g == 0) tail_g = default_tail_g(si);
     if (hash_nt < 32 || hash_nt > 1024 || hash_nt % 32 || (tail_g != 1 && tail_g != 2 && tail_g != 4)) return ST_BAD_ARG;
     if (tail_smem(set, tail_g) > SH_SMEM_MAX) return ST_BAD_ARG;
-    if (product_ctas == 0) product_ctas = 1;
+    if (product_ctas == 0) product_ctas = 2;
     if (product_ctas != 1 && product_ctas != 2) return ST_BAD_ARG;
     g_shape[si].hash_nt.store(hash_nt);
     g_shape[si].tail_g.store(tail_g);

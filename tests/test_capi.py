@@ -62,6 +62,27 @@ def test_argument_errors_without_gpu():
         M.Mayo(4)
 
 
+@pytest.mark.parametrize("s", [1, 2, 3, 5])
+def test_shared_shape_defaults_and_range(s):
+    """The shared-key launch shape is host state: defaults (CTA-pair product everywhere, four
+    signatures per sign-tail CTA for MAYO_2), a set shape read back, 0 = default, bad shapes
+    rejected."""
+    m = M.Mayo(s)
+    default = {"hash_threads": 64, "tail_instances": 4 if s == 2 else 1, "product_ctas": 2}
+    try:
+        m.set_shared_shape(0, 0, 0)
+        assert m.shared_shape() == default
+        m.set_shared_shape(128, 2, 1)
+        assert m.shared_shape() == {"hash_threads": 128, "tail_instances": 2, "product_ctas": 1}
+        for bad in ((48, 1, 1), (2048, 1, 1), (64, 3, 1), (64, 1, 3)):
+            with pytest.raises(M.MayoError):
+                m.set_shared_shape(*bad)
+        assert m.shared_shape()["hash_threads"] == 128  # a rejected shape changes nothing
+    finally:
+        m.set_shared_shape(0, 0, 0)
+    assert m.shared_shape() == default
+
+
 def test_python_mirror_has_reference_names():
     ref = ["crypto_sign_keypair", "crypto_sign_keypair_DtH", "crypto_sign_expandsk_HtD", "crypto_sign_expandsk",
            "crypto_sign_expandsk_DtH", "crypto_sign_expandpk_HtD", "crypto_sign_expandpk",
