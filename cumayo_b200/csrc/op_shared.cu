@@ -333,6 +333,56 @@ __device__ __forceinline__ bool warp_wait_armed(const uint32_t *loaded, uint32_t
     return true;
 }
 
+// The CTA's vector columns in shared memory, [KPAD/16][NINST][16]: column n = (instance n / k,
+// vector j = n % k), K byte 4 c + b' = bit b' of entry c (0 past the vectors or the batch).
+// Threads 0 .. NTH-1.  Each thread issues the loads of eight items before it stores any, so they
+// are in flight together: one item at a time (a load, then its store) the build took ~8 us per
+// CTA, on the path before the first MMA.
+template <int SET, bool VERIFY, int NTH>
+__device__ __forceinline__ void build_vector_columns(uint8_t *sB, const uint8_t *__restrict__ vec, size_t vec_stride,
+                                                     uint32_t inst0, uint32_t batch, int tid) {
+    using P = SharedProb<SET, VERIFY>;
+    using S = Set<SET>;
+    constexpr int NIN = P::NINST, ITEMS = (P::KPAD / 16) * NIN, ITER = (ITEMS + NTH - 1) / NTH, B = 8;
+#pragma unroll 1
+    for (int q0 = 0; q0 < ITER; q0 += B) {
+        uint32_t lo[B], hi[B], sh[B];
+#pragma unroll
+        for (int u = 0; u < B; u++) {
+            const int idx = tid + (q0 + u) * NTH;
+            const int ch = idx / NIN, n = idx - ch * NIN;
+            const uint32_t inst = inst0 + (uint32_t)(n / S::k);
+            const int j = n % S::k;
+            lo[u] = hi[u] = sh[u] = 0;
+            if (q0 + u < ITER && idx < ITEMS && n < P::NI * S::k && inst < batch && 4 * ch < P::NVEC) {
+                // the item's four nibbles from one little-endian word (the bytes after a vector
+                // are the next vector's, r's or the salt's, so all four exist); aligned word
+                // loads only, the second one only where the word is split
+                const int nib0 = j * P::NVEC + 4 * ch;
+                const uintptr_t a = reinterpret_cast<uintptr_t>(vec + (size_t)inst * vec_stride + (nib0 >> 1));
+                const uint32_t *w = reinterpret_cast<const uint32_t *>(a & ~uintptr_t(3));
+                sh[u] = (uint32_t)(a & 3) * 8 + (uint32_t)(nib0 & 1) * 4;
+                lo[u] = __ldg(w);
+                hi[u] = (a & 3) ? __ldg(w + 1) : 0u;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < B; u++) {
+            const int idx = tid + (q0 + u) * NTH;
+            if (q0 + u >= ITER || idx >= ITEMS) continue;
+            const int ch = idx / NIN, n = idx - ch * NIN;
+            const uint32_t x4 = __funnelshift_r(lo[u], hi[u], sh[u]);  // sh <= 3 * 8 + 4
+            uint32_t wd[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const uint32_t x = 4 * ch + q < P::NVEC ? (x4 >> (4 * q)) & 0xFu : 0u;
+                wd[q] = (x * 0x00204081u) & 0x01010101u;  // bit b' -> byte b'
+            }
+            *reinterpret_cast<uint4 *>(sB + ((size_t)ch * NIN + n) * 16) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+        }
+    }
+}
+
 // vec: instance i's vectors start at vec + i * vec_stride, entry c of vector j is nibble
 // j * NVEC + c.  planes: instance i at planes + i * PLANES, [j][row][w].
 //
@@ -445,27 +495,7 @@ __global__ void __launch_bounds__(SH_GEMM_NT, 1)
                 tc::mbar_wait(&full[ch % NCH], (ch / NCH) & 1u, SH_SPIN);
         }
     } else {
-        // vector columns: column n = (instance n / k, vector j = n % k); K byte 4 c + b' = bit b' of entry c
-        for (int idx = tid; idx < (KPAD / 16) * NIN; idx += SH_LOAD_WARP * 32) {
-            const int ch = idx / NIN, n = idx - ch * NIN;
-            const uint32_t inst = inst0 + (uint32_t)(n / S::k);
-            const int j = n % S::k;
-            uint32_t wd[4] = {0u, 0u, 0u, 0u};
-            if (n < P::NI * S::k && inst < batch && 4 * ch < P::NVEC) {
-                // the chunk's four nibbles from one little-endian word (aligned loads; the bytes
-                // after a vector are the next vector's, r's or the salt's, so all four exist)
-                const int nib0 = j * P::NVEC + 4 * ch;
-                const uint32_t x4 = ld_le32(vec + (size_t)inst * vec_stride + (nib0 >> 1)) >> ((nib0 & 1) * 4);
-#pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    if (4 * ch + q < P::NVEC) {
-                        const uint32_t x = (x4 >> (4 * q)) & 0xFu;
-                        wd[q] = (x * 0x00204081u) & 0x01010101u;  // bit b' -> byte b'
-                    }
-                }
-            }
-            *reinterpret_cast<uint4 *>(sB + ((size_t)ch * NIN + n) * 16) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
-        }
+        build_vector_columns<SET, VERIFY, SH_LOAD_WARP * 32>(sB, vec, vec_stride, inst0, batch, tid);
         tc::fence_async_smem();
         bar_sync(1, SH_LOAD_WARP * 32);  // warps 0-9: the vector columns are in place
     }
@@ -714,25 +744,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SH_GEMM_NT, 1)
                     wait_or_fail(&empty[ch % NCH], (ch / NCH) & 1u, spin, s_fail);
         }
     } else {
-        // vector columns, as in shared_gemm_kernel
-        for (int idx = tid; idx < (KPAD / 16) * NIN; idx += SH_LOAD_WARP * 32) {
-            const int ch = idx / NIN, n = idx - ch * NIN;
-            const uint32_t inst = inst0 + (uint32_t)(n / S::k);
-            const int j = n % S::k;
-            uint32_t wd[4] = {0u, 0u, 0u, 0u};
-            if (n < P::NI * S::k && inst < batch && 4 * ch < P::NVEC) {
-                const int nib0 = j * P::NVEC + 4 * ch;
-                const uint32_t x4 = ld_le32(vec + (size_t)inst * vec_stride + (nib0 >> 1)) >> ((nib0 & 1) * 4);
-#pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    if (4 * ch + q < P::NVEC) {
-                        const uint32_t x = (x4 >> (4 * q)) & 0xFu;
-                        wd[q] = (x * 0x00204081u) & 0x01010101u;  // bit b' -> byte b'
-                    }
-                }
-            }
-            *reinterpret_cast<uint4 *>(sB + ((size_t)ch * NIN + n) * 16) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
-        }
+        build_vector_columns<SET, VERIFY, SH_LOAD_WARP * 32>(sB, vec, vec_stride, inst0, batch, tid);
         tc::fence_async_smem();
         bar_sync(1, SH_LOAD_WARP * 32);  // warps 0-9: the vector columns are in place
         // the even CTA's MMAs read the odd CTA's vector columns too: tell it they are in place
