@@ -353,16 +353,20 @@ def run_ours(args, dist: Dist):
         # End to end, pipelined over the steps as a serving host would run them: step k + 1's
         # messages, offsets and lengths go up (pinned host -> the other of two device input
         # buffers, on an upload stream) while step k's kernels run, and step k's signatures and
-        # results come back (download stream) while step k + 1's run.  Every step's copies are
-        # inside the timed region; only the first upload and the last read-back are not
-        # overlapped.  The L2 flush stays between steps, after the next step's upload.
+        # results come back (download stream) while step k + 1's run, from the other of two
+        # device output buffers (a step's kernels never write a buffer still being read back).
+        # Every step's copies are inside the timed region; only the first upload and the last
+        # read-back are not overlapped.  The L2 flush stays between steps, after the next step's
+        # upload.
         d_in = [(d_msgs, d_offs, d_lens),
                 (torch.empty_like(d_msgs), torch.empty_like(d_offs), torch.empty_like(d_lens))]
+        d_out = [(sig, res), (torch.empty_like(sig), torch.empty_like(res))]  # also double-buffered
         up_st, down_st = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
 
         def e2e_run(steps):
-            done = [None, None]  # the kernels of the last step that read input buffer p
+            done = [None, None]  # the kernels of the last step that used buffers p
             uploaded = [None, None]
+            read = [None, None]  # the read-back of the last step that wrote output buffers p
 
             def upload(k):
                 p = k & 1
@@ -380,16 +384,21 @@ def run_ours(args, dist: Dist):
                 if k + 1 < steps:
                     upload(k + 1)
                 st.wait_event(uploaded[p])
+                if read[p] is not None:
+                    st.wait_event(read[p])
                 flush.fill_(1)
                 dm, do, dl = d_in[p]
-                m.sign_shared(esk, dm, sig, ws, batch, msg_off=do, msg_len=dl, stream=st)
-                m.verify_shared(epk, dm, sig, res, ws, batch, msg_off=do, msg_len=dl, stream=st)
+                so, ro = d_out[p]
+                m.sign_shared(esk, dm, so, ws, batch, msg_off=do, msg_len=dl, stream=st)
+                m.verify_shared(epk, dm, so, ro, ws, batch, msg_off=do, msg_len=dl, stream=st)
                 done[p] = torch.cuda.Event()
                 done[p].record(st)
                 down_st.wait_event(done[p])
                 with torch.cuda.stream(down_st):
-                    h_sig.copy_(sig, non_blocking=True)
-                    h_res.copy_(res, non_blocking=True)
+                    h_sig.copy_(so, non_blocking=True)
+                    h_res.copy_(ro, non_blocking=True)
+                read[p] = torch.cuda.Event()
+                read[p].record(down_st)
             fin = torch.cuda.Event()
             fin.record(down_st)
             st.wait_event(fin)
