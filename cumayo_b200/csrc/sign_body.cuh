@@ -8,8 +8,8 @@
 // No branch and no memory address depends on a value derived from the secret key; only the
 // attempt count is data dependent, as in MAYO.  In the elimination the pivot's inverse comes
 // from a shift of a 64-bit register constant and each column's factor from mask arithmetic
-// (gf16_div_from_basis), where the reference's elimination (sign.cu:48-100) branches on the
-// entries and indexes its multiplication and inverse tables with them.
+// (sign_eliminate), where the reference's elimination (sign.cu:48-100) branches on the entries
+// and indexes its multiplication and inverse tables with them.
 //
 // Why the elimination may differ from the reference's and still give identical bytes: when
 // rank A = m, the reference's pivot columns are the lexicographically first column basis of A
@@ -58,7 +58,11 @@ struct SignCfg {
     static constexpr size_t off_upk = X_IN_BS ? off_bs + (sz_bs > sz_acol ? sz_bs : sz_acol) : off_x + sz_x;
     static constexpr size_t off_mpk = off_upk + pad16((size_t)S::pairs * NW * 4);
     static constexpr size_t off_piv = off_mpk + pad16((size_t)S::k * S::o * NW * 4);
-    static constexpr size_t off_rhs = off_piv + (size_t)2 * (W + 3) * 16;
+    // pivot buffer (uint4 items, two of them: step parity): the published pivot column ([w]), the
+    // pivot row's one-hot words (2 items), the basis multiples of a_p^-1 (1 item; see sign_eliminate)
+    static constexpr int PIVQ = W + 3;
+    static_assert(W <= 8, "one-hot words fit in two items");
+    static constexpr size_t off_rhs = off_piv + (size_t)2 * PIVQ * 16;
     static constexpr size_t off_y = off_rhs + (size_t)W * 16;
     static constexpr size_t off_key = off_y + pad16(NW * 4);
     static constexpr size_t off_t = off_key + pad16(S::digest + 2 * S::sk + 1);
@@ -138,7 +142,7 @@ __device__ __forceinline__ void sign_load_ws(uint8_t *smem, int tid, const uint8
     uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
     uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
     uint32_t *mpk = reinterpret_cast<uint32_t *>(smem + C::off_mpk);  // [k][o][NW]
-    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W + 3]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][PIVQ]
     uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);     // [W]
     uint32_t *ypk = reinterpret_cast<uint32_t *>(smem + C::off_y);
     uint8_t *s_key = smem + C::off_key;  // digest || salt || seed_sk || ctr
@@ -187,7 +191,7 @@ __device__ __forceinline__ void sign_hash_cta(uint8_t *smem, int tid, const uint
     uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
     uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
     uint32_t *mpk = reinterpret_cast<uint32_t *>(smem + C::off_mpk);  // [k][o][NW]
-    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W + 3]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][PIVQ]
     uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);     // [W]
     uint32_t *ypk = reinterpret_cast<uint32_t *>(smem + C::off_y);
     uint8_t *s_key = smem + C::off_key;  // digest || salt || seed_sk || ctr
@@ -228,7 +232,7 @@ __device__ __forceinline__ void sign_next_vr(uint8_t *smem, int tid, int ctr) {
     uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
     uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
     uint32_t *mpk = reinterpret_cast<uint32_t *>(smem + C::off_mpk);  // [k][o][NW]
-    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W + 3]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][PIVQ]
     uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);     // [W]
     uint32_t *ypk = reinterpret_cast<uint32_t *>(smem + C::off_y);
     uint8_t *s_key = smem + C::off_key;  // digest || salt || seed_sk || ctr
@@ -277,7 +281,7 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem0, int T, const uint8_
     uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
     uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
     uint32_t *mpk = reinterpret_cast<uint32_t *>(smem + C::off_mpk);  // [k][o][NW]
-    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W + 3]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][PIVQ]
     uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);     // [W]
     uint32_t *ypk = reinterpret_cast<uint32_t *>(smem + C::off_y);
     uint8_t *s_key = smem + C::off_key;  // digest || salt || seed_sk || ctr
@@ -507,7 +511,7 @@ __device__ __forceinline__ bool sign_eliminate(uint8_t *smem0, int T) {
     const int tid = G == 1 ? T : T / G;
     uint8_t *smem = smem0 + (G == 1 ? 0 : (size_t)(T % G) * C::total);
     uint4 *acol = reinterpret_cast<uint4 *>(smem + C::off_bs);    // [NCOL][W]
-    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);  // [2][W + 3]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);  // [2][PIVQ]
     uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);  // [W]
     const uint8_t *s_vr = smem + C::off_vr;
     uint8_t *s_x = smem + C::off_xs;
@@ -557,13 +561,21 @@ __device__ __forceinline__ bool sign_eliminate(uint8_t *smem0, int T) {
 #pragma unroll
         for (int w = 0; w < W; w++) my_oh[q][w] = 0;
     }
-    // The owner of a column computes its pivot (lowest unpivoted row with a nonzero entry) a_p and
-    // publishes D = a + e_p, the row one-hot and the basis multiples B_s = a_p^-1 x^s in buffer
-    // pcx & 1 ([0, W) D, [W, W + 2) one-hot words, [W + 2] B); a column with entry e in row p
-    // then takes col ^= (e / a_p) D with e / a_p = sum_s e_s B_s, which is col ^= e F' with
-    // F' = a_p^-1 (a + e_p).
+    // The owner of a column computes its pivot (lowest unpivoted row with a nonzero entry) a_p; a
+    // column with entry e in row p then takes col ^= (e / a_p)(a + e_p) (eliminates row p,
+    // normalises the pivot row).  Two forms of what the owner publishes in buffer pcx & 1 (the
+    // row's one-hot words at [W, W + 2) in both):
+    //   * PREDIV (the shared-key tail, several signatures per CTA and many per SM, bound by the
+    //     ALU): D' = a_p^-1 (a + e_p) at [0, W); a column applies the masks of its own entry's
+    //     bits to the x-multiples of D' (col ^= e D'), forming no quotient.  MAYO_2 at 65,536:
+    //     1.662 -> 1.633 ms.
+    //   * otherwise (one signature per CTA, where the owner's chain sets each step's pace):
+    //     D = a + e_p at [0, W) and the basis multiples B_s = a_p^-1 x^s at [W + 2]; a column forms
+    //     e / a_p = sum_s e_s B_s by masks.  The owner's extra scalar product of the first form made
+    //     these paths ~1 % slower.
+    constexpr bool PREDIV = CP_;
     auto publish = [&](int q, int pcx) {
-        uint4 *buf = pivbuf + (pcx & 1) * (W + 3);
+        uint4 *buf = pivbuf + (pcx & 1) * C::PIVQ;
         uint32_t *ohw = reinterpret_cast<uint32_t *>(buf + W);  // oh[0..W)
         uint32_t oh[W], found = 0;
 #pragma unroll
@@ -585,17 +597,25 @@ __device__ __forceinline__ bool sign_eliminate(uint8_t *smem0, int T) {
         // a_p (0 when the column has no unpivoted nonzero entry: then oh = 0 and no column changes)
         const uint32_t piv = (uint32_t)(o0 != 0) | ((uint32_t)(o1 != 0) << 1) | ((uint32_t)(o2 != 0) << 2) |
                              ((uint32_t)(o3 != 0) << 3);
+        const uint32_t b0 = gf16_inv_reg(piv);  // a_p^-1 by a shift of a register constant
 #pragma unroll
         for (int w = 0; w < W; w++) {
             G4 ap = col[q][w];
             ap.p0 ^= oh[w];
-            g4_st(buf + w, ap);
+            if constexpr (PREDIV) {
+                G4 d = g4_zero();
+                g4_madd(d, ap, scalar_masks(b0));
+                g4_st(buf + w, d);
+            } else {
+                g4_st(buf + w, ap);
+            }
             ohw[w] = oh[w];
             my_oh[q][w] = oh[w];
         }
-        // a_p^-1 by a shift of a register constant, then x a_p^-1, x^2 a_p^-1, x^3 a_p^-1
-        const uint32_t b0 = gf16_inv_reg(piv), b1 = gf16_xtime(b0), b2 = gf16_xtime(b1), b3 = gf16_xtime(b2);
-        buf[W + 2] = make_uint4(b0, b1, b2, b3);
+        if constexpr (!PREDIV) {  // x a_p^-1, x^2 a_p^-1, x^3 a_p^-1
+            const uint32_t b1 = gf16_xtime(b0), b2 = gf16_xtime(b1), b3 = gf16_xtime(b2);
+            buf[W + 2] = make_uint4(b0, b1, b2, b3);
+        }
         my_has[q] = found;
     };
 #pragma unroll
@@ -615,7 +635,7 @@ __device__ __forceinline__ bool sign_eliminate(uint8_t *smem0, int T) {
         // be a no-op; skipping it depends only on the public loop index.  Lookahead: the owner
         // of column pc + 1 publishes its pivot right after its own update, while the other
         // columns update, so each step needs one barrier and the owner's chain overlaps them.
-        const uint4 *buf = pivbuf + (pc & 1) * (W + 3);
+        const uint4 *buf = pivbuf + (pc & 1) * C::PIVQ;
         const uint32_t *ohw = reinterpret_cast<const uint32_t *>(buf + W);
         G4 D[W];
         uint32_t oh[W];
@@ -625,7 +645,6 @@ __device__ __forceinline__ bool sign_eliminate(uint8_t *smem0, int T) {
             oh[w] = ohw[w];
             pivoted[w] |= oh[w];
         }
-        const uint4 Bp = buf[W + 2];  // a_p^-1 x^s, s = 0..3
 #pragma unroll
         for (int q = 0; q < CPT; q++) {
             const int c = KO - (tid + NT * q);
@@ -638,7 +657,13 @@ __device__ __forceinline__ bool sign_eliminate(uint8_t *smem0, int T) {
                 e2 |= col[q][w].p2 & oh[w];
                 e3 |= col[q][w].p3 & oh[w];
             }
-            const uint4 fm = scalar_masks(gf16_div_from_basis(e0, e1, e2, e3, Bp));  // e / a_p
+            uint4 fm;
+            if constexpr (PREDIV) {  // masks of e's bits (each e_s is 0 or the pivot row's one bit)
+                fm = make_uint4(0u - (uint32_t)(e0 != 0u), 0u - (uint32_t)(e1 != 0u), 0u - (uint32_t)(e2 != 0u),
+                                0u - (uint32_t)(e3 != 0u));
+            } else {  // masks of e / a_p
+                fm = scalar_masks(gf16_div_from_basis(e0, e1, e2, e3, buf[W + 2]));
+            }
 #pragma unroll
             for (int w = 0; w < W; w++) g4_madd(col[q][w], D[w], fm);
             if (c == pc + 1 && c < KO) publish(q, c);
@@ -717,7 +742,7 @@ __device__ __forceinline__ void sign_write(uint8_t *smem, int tid, const uint8_t
     uint4 *xacc = reinterpret_cast<uint4 *>(smem + C::off_x);
     uint32_t *upk = reinterpret_cast<uint32_t *>(smem + C::off_upk);
     uint32_t *mpk = reinterpret_cast<uint32_t *>(smem + C::off_mpk);  // [k][o][NW]
-    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][W + 3]
+    uint4 *pivbuf = reinterpret_cast<uint4 *>(smem + C::off_piv);     // [2][PIVQ]
     uint4 *rhsacc = reinterpret_cast<uint4 *>(smem + C::off_rhs);     // [W]
     uint32_t *ypk = reinterpret_cast<uint32_t *>(smem + C::off_y);
     uint8_t *s_key = smem + C::off_key;  // digest || salt || seed_sk || ctr
