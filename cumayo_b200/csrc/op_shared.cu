@@ -906,21 +906,27 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SH_GEMM_NT, 1)
 // 1, 2 or 4, the autotuner's candidates (4 only where the CTA fits in shared memory).
 template <int SET, int G>
 struct TailShape {
-    static constexpr int NT = SignCfg<SET>::NT * G;
+    // threads per signature: three warps where the elimination's ko + 1 columns fit (MAYO_1: 81,
+    // MAYO_2: 69); the engine's row slots shrink with them (R = 3 / 12).  More signatures per SM
+    // at the same registers: MAYO_2 G = 4, 4 CTAs of 384 threads at 40 registers (16 signatures
+    // per SM against 12 with 128 threads), 1.643 -> 1.494 ms at 65,536.
+    static constexpr int TNT = (SET == 1 || SET == 2) ? 96 : SignCfg<SET>::NT;
+    static constexpr int NT = TNT * G;
     // MAYO_5: 5 CTAs of 160 threads per SM held to a register budget (72 registers)
     // MAYO_2: the elimination's per-step chain needs signatures in flight more than registers.
-    // At 65,536: G = 1, 9 CTAs per SM (56 registers) 1.866 ms; G = 2 with 5 CTAs (48 registers)
-    // 1.739 ms (4 CTAs: 1.889, 6: 1.777); G = 4 with 3 CTAs (40 registers, 12 signatures per SM)
-    // 1.661 ms (2 CTAs: 2.055)
-    static constexpr int MINB = SET == 5 ? (G == 1 ? 5 : 2) : (SET == 2 ? (G == 1 ? 1 : G == 2 ? 5 : 3) : 1);
-    static constexpr size_t SMEM = (size_t)G * SignCfg<SET, 0, true>::total;
+    // With 128 threads per signature at 65,536: G = 1, 9 CTAs per SM (56 registers) 1.866 ms;
+    // G = 2 with 5 CTAs (48 registers) 1.739 ms (4 CTAs: 1.889, 6: 1.777); G = 4 with 3 CTAs
+    // (40 registers, 12 signatures per SM) 1.661 ms (2 CTAs: 2.055).  With 96 threads: G = 2 at 7
+    // CTAs and G = 4 at 4 CTAs per SM (the same registers).
+    static constexpr int MINB = SET == 5 ? (G == 1 ? 5 : 2) : (SET == 2 ? (G == 1 ? 1 : G == 2 ? 7 : 4) : 1);
+    static constexpr size_t SMEM = (size_t)G * SignCfg<SET, TNT, true>::total;
 };
 template <int SET, int G>
 __global__ void __launch_bounds__(TailShape<SET, G>::NT, TailShape<SET, G>::MINB)
     sign_shared_tail_kernel(const uint8_t *esk, uint8_t *sig, size_t sig_stride, const uint8_t *wsi, size_t wsi_stride,
                             const uint4 *planes, const uint4 *opl, uint32_t *ctl, uint32_t *retry, uint32_t batch) {
     using P = SharedProb<SET, false>;
-    using C = SignCfg<SET, 0, true>;
+    using C = SignCfg<SET, TailShape<SET, G>::TNT, true>;
     constexpr int NT = C::NT;
     extern __shared__ __align__(16) uint8_t smem0[];
     if (ctl[0]) return;  // the product gave up: the fix-up kernel signs everything
@@ -1263,8 +1269,8 @@ int shared_timing_read(float *ms) {
 // Shared memory a sign-tail CTA of g instances needs (0 for a bad set).
 static size_t tail_smem(int set, int g) {
     switch (set) {
-        case 1: return (size_t)g * SignCfg<1, 0, true>::total;
-        case 2: return (size_t)g * SignCfg<2, 0, true>::total;
+        case 1: return (size_t)g * SignCfg<1, TailShape<1, 1>::TNT, true>::total;
+        case 2: return (size_t)g * SignCfg<2, TailShape<2, 1>::TNT, true>::total;
         case 3: return (size_t)g * SignCfg<3, 0, true>::total;
         case 5: return (size_t)g * SignCfg<5, 0, true>::total;
         default: return 0;

@@ -39,8 +39,10 @@ template <int SET, int NT_ = 0, bool COMPACT = false>
 struct SignCfg {
     using S = Set<SET>;
     static constexpr int J = S::k, W = S::W;
-    static constexpr int R = SET == 2 ? 16 : (SET == 1 ? 4 : 2);
     static constexpr int NT = NT_ ? NT_ : (SET == 5 ? 160 : 128);
+    // engine row slots: J * W * R threads run the engine, so fewer threads get fewer slots
+    static constexpr int R0 = SET == 2 ? 16 : (SET == 1 ? 4 : 2);
+    static constexpr int R = NT / (J * W) < R0 ? NT / (J * W) : R0;
     static constexpr int NCOL = S::ko + 1;  // columns of [A | y]
     static constexpr int CPT = (NCOL + NT - 1) / NT;
     static constexpr int NW = (S::menc + 3) / 4;
