@@ -1114,8 +1114,10 @@ struct SharedShape {
 };
 // Defaults (MAYO_1, 2, 3, 5), measured at 65,536 instances: the pair product is the faster one
 // for every set (MAYO_5 sign 14.0 against 18.5 ms: one CTA's key ring holds only four chunks
-// beside its vectors), and four signatures per sign-tail CTA pay only for MAYO_2.
-constexpr int default_tail_g(int si) { return si == 1 ? 4 : 1; }
+// beside its vectors); signatures per sign-tail CTA: four for MAYO_2 (1.494 ms against 1.631 with
+// two, 1.840 with one), two for MAYO_1 (5.12 ms against 7.11 with one, 8.22 with four), one for
+// MAYO_3 and MAYO_5 (13.49 / 29.73 ms against 14.62 / 36.03 with two).
+constexpr int default_tail_g(int si) { return si == 1 ? 4 : si == 0 ? 2 : 1; }
 SharedShape g_shape[4] = {{HASH_NT, default_tail_g(0), 1}, {HASH_NT, default_tail_g(1), 1},
                           {HASH_NT, default_tail_g(2), 1}, {HASH_NT, default_tail_g(3), 1}};
 static int shape_index(int set) { return set == 1 ? 0 : set == 2 ? 1 : set == 3 ? 2 : set == 5 ? 3 : -1; }

@@ -193,11 +193,11 @@ MAYO_B200_API int mayo_b200_shared_timing(int enable);
 /* Launch shape of the shared-key calls of one parameter set, process-wide (set it before the
  * calls it should apply to; calls already issued keep theirs).  hash_threads: threads per CTA
  * of the thread-per-instance hash kernels (a multiple of 32, 32..1024; 0 = 64); tail_instances:
- * signatures per CTA of the sign tail (1, 2 or 4; 0 = 4 for MAYO_2, else 1; with more than one
- * the instances' elimination columns are interleaved over the CTA's warps); product_ctas: CTAs
- * per tile of the tensor-core key product (1, or 2: a cluster of two CTAs on two SMs running
- * cta_group::2 MMAs, each SM streaming half of every key tile; 0 = 2).  The defaults hold until
- * a shape is set.  Results do not depend on the shape;
+ * signatures per CTA of the sign tail (1, 2 or 4; 0 = 4 for MAYO_2, 2 for MAYO_1, else 1; with
+ * more than one the instances' elimination columns are interleaved over the CTA's warps);
+ * product_ctas: CTAs per tile of the tensor-core key product (1, or 2: a cluster of two CTAs on
+ * two SMs running cta_group::2 MMAs, each SM streaming half of every key tile; 0 = 2).  The
+ * defaults hold until a shape is set.  Results do not depend on the shape;
  * cumayo_b200.autotune times the candidates.  MAYO_B200_ERR_ARG for a shape out of range or
  * one whose CTA would not fit in shared memory; shape NULL = the defaults. */
 typedef struct mayo_b200_shared_shape {

@@ -65,10 +65,10 @@ def test_argument_errors_without_gpu():
 @pytest.mark.parametrize("s", [1, 2, 3, 5])
 def test_shared_shape_defaults_and_range(s):
     """The shared-key launch shape is host state: defaults (CTA-pair product everywhere, four
-    signatures per sign-tail CTA for MAYO_2), a set shape read back, 0 = default, bad shapes
-    rejected."""
+    signatures per sign-tail CTA for MAYO_2, two for MAYO_1), a set shape read back, 0 = default,
+    bad shapes rejected."""
     m = M.Mayo(s)
-    default = {"hash_threads": 64, "tail_instances": 4 if s == 2 else 1, "product_ctas": 2}
+    default = {"hash_threads": 64, "tail_instances": {1: 2, 2: 4}.get(s, 1), "product_ctas": 2}
     try:
         m.set_shared_shape(0, 0, 0)
         assert m.shared_shape() == default
