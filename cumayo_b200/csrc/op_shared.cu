@@ -996,7 +996,11 @@ __global__ void verify_hash_kernel(const VerifyIO io, uint8_t *tws, size_t tws_s
 template <int SET>
 struct VTailCfg {
     using S = Set<SET>;
-    static constexpr int J = S::k, W = S::W, NW = (S::menc + 3) / 4, NT = 128;
+    // threads per verification, measured at 65,536: MAYO_1 96 (2.18 ms against 2.26 with 128, 3.25
+    // with 256), MAYO_2 96 (0.279 against 0.291, 0.309 with 64), MAYO_3 128 (5.14 against 5.23 with
+    // 96, 5.35 with 256), MAYO_5 256 (8.90 against 9.62 with 128, 15.5 with 64)
+    static constexpr int J = S::k, W = S::W, NW = (S::menc + 3) / 4,
+                         NT = SET == 5 ? 256 : SET == 3 ? 128 : 96;
     static constexpr int R = NT / (J * W);
     static_assert(R >= 1, "verify tail threads");
     static constexpr size_t off_masks = 0;
