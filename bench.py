@@ -68,11 +68,13 @@ KERNEL_ROOF_DEF = {
 }
 # DRAM bytes per instance (dram__bytes_read.sum + dram__bytes_write.sum of one launch / its
 # instances) from ncu captures of the MAYO_2 shared-key kernels at 16,384 instances (the sign
-# tail with four signatures per CTA: profiles/sign_tail_mayo2_shared_b16384.md; the others:
-# profiles/product_gemm_mayo2_shared_b16384.md);
-# the traffic grows in proportion to the instances, so a launch's traffic is this x its batch.
-KERNEL_TRAFFIC_PER_INST = {2: {"sign.tail": (174.092288e6 + 4.834816e6) / 16384, "verify.tail": 177.242624e6 / 16384,
-                               "sign.product": 130.477568e6 / 16384, "verify.product": 128.245248e6 / 16384}}
+# tail with four signatures per CTA: profiles/sign_tail_mayo2_shared_b16384.md; the products on
+# CTA pairs: profiles/product_gemm_mayo2_shared_b16384.md; the verify tail from an earlier
+# capture of the same command); the traffic grows in proportion to the instances, so a launch's
+# traffic is this x its batch.
+KERNEL_TRAFFIC_PER_INST = {2: {"sign.tail": (174.092544e6 + 4.883456e6) / 16384, "verify.tail": 177.242624e6 / 16384,
+                               "sign.product": (11.437568e6 + 118.18368e6) / 16384,
+                               "verify.product": (10.445568e6 + 119.318528e6) / 16384}}
 # The same for verify_kernel<SET> on distinct keys (one capture of 4,096 instances per set,
 # profiles/verify_distinct_mayo3_mayo5_b4096.md): the instance's EPK is read once.
 VERIFY_TRAFFIC_PER_INST = {3: (1.557413e9 + 4.978176e6) / 4096, 5: (3.478466e9 + 4.699392e6) / 4096}
