@@ -339,15 +339,16 @@ __device__ __forceinline__ bool warp_wait_armed(const uint32_t *loaded, uint32_t
 
 // The CTA's vector columns in shared memory, [KPAD/16][NINST][16]: column n = (instance n / k,
 // vector j = n % k), K byte 4 c + b' = bit b' of entry c (0 past the vectors or the batch).
-// Threads 0 .. NTH-1.  Each thread issues the loads of eight items before it stores any, so they
-// are in flight together: one item at a time (a load, then its store) the build took ~8 us per
-// CTA, on the path before the first MMA.
+// Threads 0 .. NTH-1.  Each thread issues the loads of up to 24 items before it stores any, so
+// they are in flight together (MAYO_1/2/3: all of a thread's items, one round of memory latency):
+// the build is on the path before the first MMA (3.6 / 5.0 us of a MAYO_2 sign / verify pair
+// CTA's 87 / 98 us with eight in flight; 0.616 -> 0.611 ms and 0.695 -> 0.684 ms with 24).
 template <int SET, bool VERIFY, int NTH>
 __device__ __forceinline__ void build_vector_columns(uint8_t *sB, const uint8_t *__restrict__ vec, size_t vec_stride,
                                                      uint32_t inst0, uint32_t batch, int tid) {
     using P = SharedProb<SET, VERIFY>;
     using S = Set<SET>;
-    constexpr int NIN = P::NINST, ITEMS = (P::KPAD / 16) * NIN, ITER = (ITEMS + NTH - 1) / NTH, B = 8;
+    constexpr int NIN = P::NINST, ITEMS = (P::KPAD / 16) * NIN, ITER = (ITEMS + NTH - 1) / NTH, B = ITER < 24 ? ITER : 24;
 #pragma unroll 1
     for (int q0 = 0; q0 < ITER; q0 += B) {
         uint32_t lo[B], hi[B], sh[B];
