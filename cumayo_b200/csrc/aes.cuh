@@ -3,11 +3,13 @@
 // 0^8 || BE64(i), output bytes in standard AES order, a final partial block keeps its leading
 // bytes.
 //
-// B200 layout: one round table T0 (Te0 of FIPS-197 in big-endian words) replicated 32 times in
+// B200 layout: the round table T0 (Te0 of FIPS-197 in big-endian words) replicated 32 times in
 // shared memory, entry x of copy c at word 32*x + c, so lane c always hits bank c and the 16
-// data-dependent lookups of a round never conflict.  The other three tables are byte rotations
-// of T0 (PRMT).  The S-box for the last round is byte 1 of T0[x].  Tables are computed at compile
-// time from GF(2^8) arithmetic.
+// data-dependent lookups of a round never conflict.  The other three round tables are byte
+// rotations of T0.  The expansion kernel keeps T0, ror8(T0) and ror16(T0) (96 KB, two CTAs of 384
+// threads per SM) and rotates only for the fourth; the work-queue kernel keeps T0 alone (32 KB)
+// and rotates with PRMT.  The S-box for the last round is byte 1 of T0[x].  Tables are computed at
+// compile time from GF(2^8) arithmetic.
 #pragma once
 
 #include "common.cuh"
@@ -63,8 +65,10 @@ __device__ __forceinline__ uint32_t ror16(uint32_t x) { return __byte_perm(x, x,
 __device__ __forceinline__ uint32_t ror24(uint32_t x) { return __byte_perm(x, x, 0x2103); }
 __device__ __forceinline__ uint32_t byte_of(uint32_t x, int b) { return __byte_perm(x, 0, 0x4440 | b); }
 
-// AES-128 key schedule (FIPS-197 5.2) from 16 key bytes at any address.
-__device__ inline void aes128_key_schedule(const uint8_t *key, uint32_t *rk) {
+// AES-128 key schedule (FIPS-197 5.2) from 16 key bytes at any address; `sb` is the S-box (the
+// constant-memory copy by default, a shared-memory copy where threads look up different bytes).
+__device__ inline void aes128_key_schedule(const uint8_t *key, uint32_t *rk, const uint8_t *sb = nullptr) {
+    if (!sb) sb = c_aes.sbox;
 #pragma unroll
     for (int i = 0; i < 4; i++)
         rk[i] = ((uint32_t)key[4 * i] << 24) | ((uint32_t)key[4 * i + 1] << 16) | ((uint32_t)key[4 * i + 2] << 8) |
@@ -75,8 +79,8 @@ __device__ inline void aes128_key_schedule(const uint8_t *key, uint32_t *rk) {
         uint32_t t = rk[i - 1];
         if (i % 4 == 0) {
             t = (t << 8) | (t >> 24);
-            t = ((uint32_t)c_aes.sbox[t >> 24] << 24) | ((uint32_t)c_aes.sbox[(t >> 16) & 0xFF] << 16) |
-                ((uint32_t)c_aes.sbox[(t >> 8) & 0xFF] << 8) | c_aes.sbox[t & 0xFF];
+            t = ((uint32_t)sb[t >> 24] << 24) | ((uint32_t)sb[(t >> 16) & 0xFF] << 16) |
+                ((uint32_t)sb[(t >> 8) & 0xFF] << 8) | sb[t & 0xFF];
             t ^= rcon << 24;
             rcon = gf256_mulc((uint8_t)rcon, 2);
         }
@@ -123,6 +127,59 @@ __device__ __forceinline__ AesOut aes128_ctr_block(const uint32_t *T, const RK &
     return o;
 }
 
+// The same block with three replicated tables in shared memory: T0, ror8(T0) and ror16(T0) at
+// byte offsets 0, 32 KB and 64 KB from `base` (this lane's column already added), the fourth
+// table as ror8 of the third.  A lookup is a byte extraction, one IMAD for the address and the
+// read; the multiplier `k128` (= 128, the table stride) is a kernel argument so that the address
+// arithmetic stays on the IMAD pipe instead of joining the extractions, rotations and XORs on the
+// logic pipe, which with the table reads sets the pace (measured at MAYO_1's 1,024 x 9,031
+// blocks: one table with PRMT rotations 0.250 ms, three tables 0.203 ms, byte-exact).
+template <class RK>
+__device__ __forceinline__ AesOut aes128_ctr_block3(uint32_t base, const RK &rk, uint32_t blk, uint32_t k128) {
+    auto t0 = [&](uint32_t x) {
+        uint32_t v;
+        asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(x * k128 + base));
+        return v;
+    };
+    auto t1 = [&](uint32_t x) {
+        uint32_t v;
+        asm volatile("ld.shared.u32 %0, [%1+32768];" : "=r"(v) : "r"(x * k128 + base));
+        return v;
+    };
+    auto t2 = [&](uint32_t x) {
+        uint32_t v;
+        asm volatile("ld.shared.u32 %0, [%1+65536];" : "=r"(v) : "r"(x * k128 + base));
+        return v;
+    };
+    uint32_t s0 = rk[0], s1 = rk[1], s2 = rk[2], s3 = blk ^ rk[3];
+#pragma unroll
+    for (int r = 1; r < 10; r++) {
+        const uint32_t t0w = t0(s0 >> 24) ^ t1(byte_of(s1, 2)) ^ t2(byte_of(s2, 1)) ^ ror8(t2(byte_of(s3, 0))) ^ rk[4 * r];
+        const uint32_t t1w =
+            t0(s1 >> 24) ^ t1(byte_of(s2, 2)) ^ t2(byte_of(s3, 1)) ^ ror8(t2(byte_of(s0, 0))) ^ rk[4 * r + 1];
+        const uint32_t t2w =
+            t0(s2 >> 24) ^ t1(byte_of(s3, 2)) ^ t2(byte_of(s0, 1)) ^ ror8(t2(byte_of(s1, 0))) ^ rk[4 * r + 2];
+        const uint32_t t3w =
+            t0(s3 >> 24) ^ t1(byte_of(s0, 2)) ^ t2(byte_of(s1, 1)) ^ ror8(t2(byte_of(s2, 0))) ^ rk[4 * r + 3];
+        s0 = t0w;
+        s1 = t1w;
+        s2 = t2w;
+        s3 = t3w;
+    }
+    // last round: S-box = byte 1 of T0[x]
+#define LASTW(a, b, c, d, k)                                                                   \
+    (__byte_perm(__byte_perm(t0((a) >> 24), t0(byte_of(b, 2)), 0x1500),                         \
+                 __byte_perm(t0(byte_of(c, 1)), t0(byte_of(d, 0)), 0x0015), 0x3254) ^            \
+     rk[k])
+    AesOut o;
+    o.w0 = LASTW(s0, s1, s2, s3, 40);
+    o.w1 = LASTW(s1, s2, s3, s0, 41);
+    o.w2 = LASTW(s2, s3, s0, s1, 42);
+    o.w3 = LASTW(s3, s0, s1, s2, 43);
+#undef LASTW
+    return o;
+}
+
 // Big-endian words -> little-endian words of the byte stream.
 __device__ __forceinline__ uint32_t bswap32(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
 
@@ -148,74 +205,90 @@ __device__ __forceinline__ void st16(uint8_t *p, uint32_t a, uint32_t b, uint32_
 }
 
 // ---------------------------------------------------------------------------------------------
-// Kernel: AES-CTR keystream into a pitched pool.  grid = (chunks, batch); blocks
-// [0, nblk_main) of instance blockIdx.y go to row + out_off, keyed by 16 bytes at row + key_off.
-// When the key overlaps the output (expand-pk, expand-sk keep seed_pk in the last 16 output
-// bytes until expansion), nblk_main excludes the blocks that overlap the key and
-// aes_ctr_tail_kernel finishes them afterwards, one thread per instance.
+// Kernel: AES-CTR keystream into a pitched pool.  grid = (chunks, batch); chunk x of instance
+// blockIdx.y takes blocks [x * bpc, min((x + 1) * bpc, nblk_main)) to row + out_off, keyed by 16
+// bytes at row + key_off.  The launcher splits an instance's blocks into near-equal chunks of at
+// most AES_BLOCKS_PER_CTA.  When the key overlaps the output (expand-pk, expand-sk keep seed_pk
+// in the last 16 output bytes until expansion), nblk_main excludes the blocks that overlap the
+// key and aes_ctr_tail_kernel finishes them afterwards, one thread per instance.
 // ---------------------------------------------------------------------------------------------
-constexpr int AES_THREADS = 256;
-constexpr int AES_BLOCKS_PER_CTA = 2048;
+constexpr int AES_THREADS = 384;
+constexpr int AES_BLOCKS_PER_CTA = 3072;
+constexpr size_t AES_SMEM = 3 * 256 * 32 * 4;  // T0, ror8(T0), ror16(T0), each replicated 32 times
 
-static __global__ void __launch_bounds__(AES_THREADS) aes_ctr_kernel(uint8_t *pool, size_t pitch, size_t key_off,
-                                                               size_t out_off, uint32_t nblk_main) {
-    extern __shared__ uint32_t aes_smem[];  // 256 * 32 words
+static __global__ void __launch_bounds__(AES_THREADS, 2)
+    aes_ctr_kernel(uint8_t *pool, size_t pitch, size_t key_off, size_t out_off, uint32_t nblk_main, uint32_t bpc,
+                   uint32_t k128) {
+    extern __shared__ uint32_t aes_smem[];  // [3][256 * 32] words
     __shared__ uint32_t rk_s[44];
     uint8_t *row = pool + (size_t)blockIdx.y * pitch;
-    for (int i = threadIdx.x; i < 256 * 32; i += AES_THREADS) aes_smem[i] = c_aes.te0[i >> 5];
+    for (int i = threadIdx.x; i < 256 * 32; i += AES_THREADS) {
+        const uint32_t v = c_aes.te0[i >> 5];
+        aes_smem[i] = v;
+        aes_smem[256 * 32 + i] = ror8(v);
+        aes_smem[2 * 256 * 32 + i] = ror16(v);
+    }
     if (threadIdx.x == 0) aes128_key_schedule(row + key_off, rk_s);
     __syncthreads();
     uint32_t rk[44];
 #pragma unroll
     for (int i = 0; i < 44; i++) rk[i] = rk_s[i];
-    const uint32_t *T = aes_smem + (threadIdx.x & 31);
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(aes_smem + (threadIdx.x & 31));
     uint8_t *out = row + out_off;
-    const uint32_t b0 = blockIdx.x * AES_BLOCKS_PER_CTA;
-    const uint32_t b1 = min(b0 + AES_BLOCKS_PER_CTA, nblk_main);
+    const uint32_t b0 = blockIdx.x * bpc;
+    const uint32_t b1 = min(b0 + bpc, nblk_main);
     for (uint32_t blk = b0 + threadIdx.x; blk < b1; blk += AES_THREADS) {
-        AesOut o = aes128_ctr_block(T, rk, blk);
+        AesOut o = aes128_ctr_block3(base, rk, blk, k128);
         st16(out + (size_t)blk * 16, bswap32(o.w0), bswap32(o.w1), bswap32(o.w2), bswap32(o.w3));
     }
 }
 
 // Blocks [nblk_main, ceil(nbytes/16)) for each instance (key read before any byte is written).
-static __global__ void aes_ctr_tail_kernel(uint8_t *pool, size_t pitch, size_t key_off, size_t out_off,
-                                    uint32_t nblk_main, uint32_t nbytes, uint32_t batch) {
-    uint32_t inst = blockIdx.x * blockDim.x + threadIdx.x;
+// One thread per instance, at most two blocks each; the threads of a warp look up different
+// bytes, so the tables are copied to shared memory first (constant memory would serialise them).
+constexpr int AES_TAIL_THREADS = 128;
+static __global__ void __launch_bounds__(AES_TAIL_THREADS)
+    aes_ctr_tail_kernel(uint8_t *pool, size_t pitch, size_t key_off, size_t out_off, uint32_t nblk_main,
+                        uint32_t nbytes, uint32_t batch) {
+    __shared__ uint32_t te[256];
+    __shared__ uint8_t sb[256];
+    for (int i = threadIdx.x; i < 256; i += AES_TAIL_THREADS) {
+        te[i] = c_aes.te0[i];
+        sb[i] = c_aes.sbox[i];
+    }
+    __syncthreads();
+    const uint32_t inst = blockIdx.x * blockDim.x + threadIdx.x;
     if (inst >= batch) return;
     uint8_t *row = pool + (size_t)inst * pitch;
     uint32_t rk[44];
-    aes128_key_schedule(row + key_off, rk);
+    aes128_key_schedule(row + key_off, rk, sb);
     const uint32_t nblk = (nbytes + 15) / 16;
     uint8_t buf[32];
     for (uint32_t blk = nblk_main; blk < nblk; blk++) {
-        uint32_t s[4] = {0, 0, 0, blk};
-        // plain table walk through constant memory (at most two blocks per instance)
-        uint32_t s0 = s[0] ^ rk[0], s1 = s[1] ^ rk[1], s2 = s[2] ^ rk[2], s3 = s[3] ^ rk[3];
+        uint32_t s0 = rk[0], s1 = rk[1], s2 = rk[2], s3 = blk ^ rk[3];
         for (int r = 1; r < 10; r++) {
-            uint32_t t0 = c_aes.te0[s0 >> 24] ^ ror8(c_aes.te0[(s1 >> 16) & 255]) ^
-                          ror16(c_aes.te0[(s2 >> 8) & 255]) ^ ror24(c_aes.te0[s3 & 255]) ^ rk[4 * r];
-            uint32_t t1 = c_aes.te0[s1 >> 24] ^ ror8(c_aes.te0[(s2 >> 16) & 255]) ^
-                          ror16(c_aes.te0[(s3 >> 8) & 255]) ^ ror24(c_aes.te0[s0 & 255]) ^ rk[4 * r + 1];
-            uint32_t t2 = c_aes.te0[s2 >> 24] ^ ror8(c_aes.te0[(s3 >> 16) & 255]) ^
-                          ror16(c_aes.te0[(s0 >> 8) & 255]) ^ ror24(c_aes.te0[s1 & 255]) ^ rk[4 * r + 2];
-            uint32_t t3 = c_aes.te0[s3 >> 24] ^ ror8(c_aes.te0[(s0 >> 16) & 255]) ^
-                          ror16(c_aes.te0[(s1 >> 8) & 255]) ^ ror24(c_aes.te0[s2 & 255]) ^ rk[4 * r + 3];
+            const uint32_t t0 = te[s0 >> 24] ^ ror8(te[(s1 >> 16) & 255]) ^ ror16(te[(s2 >> 8) & 255]) ^
+                                ror24(te[s3 & 255]) ^ rk[4 * r];
+            const uint32_t t1 = te[s1 >> 24] ^ ror8(te[(s2 >> 16) & 255]) ^ ror16(te[(s3 >> 8) & 255]) ^
+                                ror24(te[s0 & 255]) ^ rk[4 * r + 1];
+            const uint32_t t2 = te[s2 >> 24] ^ ror8(te[(s3 >> 16) & 255]) ^ ror16(te[(s0 >> 8) & 255]) ^
+                                ror24(te[s1 & 255]) ^ rk[4 * r + 2];
+            const uint32_t t3 = te[s3 >> 24] ^ ror8(te[(s0 >> 16) & 255]) ^ ror16(te[(s1 >> 8) & 255]) ^
+                                ror24(te[s2 & 255]) ^ rk[4 * r + 3];
             s0 = t0;
             s1 = t1;
             s2 = t2;
             s3 = t3;
         }
-        const uint8_t *S = c_aes.sbox;
         uint32_t o[4];
-        o[0] = ((uint32_t)S[s0 >> 24] << 24 | (uint32_t)S[(s1 >> 16) & 255] << 16 | (uint32_t)S[(s2 >> 8) & 255] << 8 |
-                S[s3 & 255]) ^ rk[40];
-        o[1] = ((uint32_t)S[s1 >> 24] << 24 | (uint32_t)S[(s2 >> 16) & 255] << 16 | (uint32_t)S[(s3 >> 8) & 255] << 8 |
-                S[s0 & 255]) ^ rk[41];
-        o[2] = ((uint32_t)S[s2 >> 24] << 24 | (uint32_t)S[(s3 >> 16) & 255] << 16 | (uint32_t)S[(s0 >> 8) & 255] << 8 |
-                S[s1 & 255]) ^ rk[42];
-        o[3] = ((uint32_t)S[s3 >> 24] << 24 | (uint32_t)S[(s0 >> 16) & 255] << 16 | (uint32_t)S[(s1 >> 8) & 255] << 8 |
-                S[s2 & 255]) ^ rk[43];
+        o[0] = ((uint32_t)sb[s0 >> 24] << 24 | (uint32_t)sb[(s1 >> 16) & 255] << 16 | (uint32_t)sb[(s2 >> 8) & 255] << 8 |
+                sb[s3 & 255]) ^ rk[40];
+        o[1] = ((uint32_t)sb[s1 >> 24] << 24 | (uint32_t)sb[(s2 >> 16) & 255] << 16 | (uint32_t)sb[(s3 >> 8) & 255] << 8 |
+                sb[s0 & 255]) ^ rk[41];
+        o[2] = ((uint32_t)sb[s2 >> 24] << 24 | (uint32_t)sb[(s3 >> 16) & 255] << 16 | (uint32_t)sb[(s0 >> 8) & 255] << 8 |
+                sb[s1 & 255]) ^ rk[42];
+        o[3] = ((uint32_t)sb[s3 >> 24] << 24 | (uint32_t)sb[(s0 >> 16) & 255] << 16 | (uint32_t)sb[(s1 >> 8) & 255] << 8 |
+                sb[s2 & 255]) ^ rk[43];
         for (int i = 0; i < 16; i++) buf[(blk - nblk_main) * 16 + i] = (uint8_t)(o[i >> 2] >> (24 - 8 * (i & 3)));
     }
     // write only after every tail block is computed (the key may sit in these bytes)

@@ -25,7 +25,7 @@ namespace mayo {
 // Packed bytes [p, p + n) (n <= 16) of an m-vector group as four LE words, touching only
 // aligned 32-bit words that contain at least one requested byte.  RO selects the read-only
 // (non-coherent) load path, valid only for data no thread writes during the kernel.
-template <bool RO = true>
+template <bool RO = true, bool GLOBAL = false>
 __device__ __forceinline__ void load_group_words(const uint8_t *p, int n, uint32_t &w0, uint32_t &w1, uint32_t &w2,
                                                  uint32_t &w3) {
     const uintptr_t a = reinterpret_cast<uintptr_t>(p);
@@ -34,8 +34,10 @@ __device__ __forceinline__ void load_group_words(const uint8_t *p, int n, uint32
     // number of aligned words covering [p, p + n)
     const int nw = (int)(((a & 3) + n + 3) >> 2);
     uint32_t x[5];
+    // GLOBAL: the entry is known to be in global memory; the explicit global load (L1-cached,
+    // coherent) lets the compiler issue it ahead of earlier shared-memory stores
 #pragma unroll
-    for (int i = 0; i < 5; i++) x[i] = i < nw ? (RO ? __ldg(q + i) : q[i]) : 0u;
+    for (int i = 0; i < 5; i++) x[i] = i < nw ? (RO ? __ldg(q + i) : GLOBAL ? __ldca(q + i) : q[i]) : 0u;
     w0 = __funnelshift_r(x[0], x[1], sh);
     w1 = __funnelshift_r(x[1], x[2], sh);
     w2 = __funnelshift_r(x[2], x[3], sh);
@@ -112,7 +114,8 @@ struct EngineSmem {
 // X4: row products with four partial sums (row_product_x4, measured 3-4 % faster keypair, sign
 // and verify at 1,024 instances, 4 % on the mixed queue); off where a kernel's register budget
 // leaves no room for the twelve extra live registers.
-template <int SET, int J, int R, bool X4 = true>
+// CU: groups whose loads a thread issues together in convert (1: one group at a time).
+template <int SET, int J, int R, bool X4 = true, int CU = 1>
 struct Engine {
     using S = Set<SET>;
     static constexpr int W = S::W;
@@ -134,20 +137,47 @@ struct Engine {
         rs = t / (J * W);
     }
 
-    // Convert rows [r0, r0 + R) (those < nrows) into bs; all `nthreads` threads take part.
+    // Convert rows [r0, r0 + R) (those < nrows) into bs; all `nthreads` threads take part.  With
+    // CU > 1 a thread issues the loads of CU groups (entries in global memory only) before it
+    // converts and stores any of them, so that CU round trips to L2 / HBM overlap.
     template <class Rows>
     __device__ __forceinline__ void convert(const Rows &rows, int r0, int nrows, int tid, int nthreads) {
+        constexpr bool RO = RowsReadOnly<Rows>::value;
 #pragma unroll 1
         for (int slot = 0; slot < R; slot++) {
             const int r = r0 + slot;
             if (r >= nrows) break;
-            const int cnt = rows.count(r);
+            const int n = rows.count(r) * W;
             uint4 *dst = bs + (size_t)slot * MAXE * W;
-            for (int idx = tid; idx < cnt * W; idx += nthreads) {
-                const int e = idx / W, ww = idx - e * W;
-                const uint8_t *src = rows.entry(r, e);
-                G4 g = src ? load_group<SET, RowsReadOnly<Rows>::value>(src, ww) : g4_zero();
-                g4_st(dst + idx, g);
+            if constexpr (CU == 1) {
+                for (int idx = tid; idx < n; idx += nthreads) {
+                    const int e = idx / W, ww = idx - e * W;
+                    const uint8_t *src = rows.entry(r, e);
+                    G4 g = src ? load_group<SET, RO>(src, ww) : g4_zero();
+                    g4_st(dst + idx, g);
+                }
+            } else {
+#pragma unroll 1
+                for (int i0 = tid; i0 < n; i0 += CU * nthreads) {
+                    uint32_t x[CU][4];
+#pragma unroll
+                    for (int u = 0; u < CU; u++) {
+                        const int idx = i0 + u * nthreads;
+                        x[u][0] = x[u][1] = x[u][2] = x[u][3] = 0u;
+                        if (idx < n) {
+                            const int e = idx / W, ww = idx - e * W;
+                            const uint8_t *src = rows.entry(r, e);
+                            if (src)
+                                load_group_words<RO, true>(src + 16 * ww, group_bytes<S::menc>(ww), x[u][0], x[u][1],
+                                                           x[u][2], x[u][3]);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < CU; u++) {
+                        const int idx = i0 + u * nthreads;
+                        if (idx < n) g4_st(dst + idx, g4_from_packed(x[u][0], x[u][1], x[u][2], x[u][3]));
+                    }
+                }
             }
         }
     }

@@ -71,7 +71,7 @@ struct LRows {  // row r of P1 + P1^T without the diagonal, then P2 row r (src/e
 
 // P3 = Upper(O^T (P1 O + P2)) for one instance: O (o_bytes) already in smem at off_o; writes the
 // packed upper triangle to P3out.  All NT threads must call it.  RO: P1/P2 read-only in this kernel.
-template <int SET, int NT_, bool RO>
+template <int SET, int NT_, bool RO, int CU = 1>
 __device__ __forceinline__ void p3_instance(uint8_t *smem, int tid, const uint8_t *P1, const uint8_t *P2,
                                             uint8_t *P3out) {
     using S = Set<SET>;
@@ -85,7 +85,7 @@ __device__ __forceinline__ void p3_instance(uint8_t *smem, int tid, const uint8_
     build_o_masks<SET>(masks, s_O, tid, NT);
     __syncthreads();
 
-    Engine<SET, J, R> eng;
+    Engine<SET, J, R, true, CU> eng;
     eng.setup(masks, bs, tid);
     const P3Rows<SET, RO> rows{P1, P2};
     G4 X[J];

@@ -74,7 +74,9 @@ __global__ void __launch_bounds__(KeyCfg<SET>::NT) p3_kernel(uint8_t *pool, size
     // O is parked in pk[16:]: copy it to shared memory before P3 overwrites that region
     for (int i = tid; i < S::o_bytes; i += C::NT) smem[C::off_o + i] = pk[16 + i];
     __syncthreads();
-    p3_instance<SET, C::NT, true>(smem, tid, P1, P1 + S::p1, pk + 16);
+    // batched row loads (CU = 4) measured faster for MAYO_2's P3 only (MAYO_1/3/5: 0.494 -> 0.502,
+    // 1.18 -> 1.20, 2.89 -> 3.04 ms per 1,024 keypairs; MAYO_2 0.475 -> 0.462)
+    p3_instance<SET, C::NT, true, SET == 2 ? 4 : 1>(smem, tid, P1, P1 + S::p1, pk + 16);
 }
 
 template <int SET>
@@ -96,7 +98,10 @@ __global__ void __launch_bounds__(KeyCfg<SET>::NT) l_kernel(uint8_t *pool, size_
     build_o_masks<SET>(masks, s_O, tid, NT);
     __syncthreads();
 
-    Engine<SET, J, R> eng;
+    // four row groups' loads in flight per thread: L reads P1 twice (rows and columns) with
+    // little else to hide the latency (MAYO_1 signWithesk 1.10 -> 1.07 ms per 1,024, MAYO_5
+    // 7.13 -> 6.97)
+    Engine<SET, J, R, true, 4> eng;
     eng.setup(masks, bs, tid);
     const LRows<SET> rows{P1, P2};
 #pragma unroll 1
@@ -122,12 +127,16 @@ static int aes_expand(uint8_t *pool, size_t pitch, size_t batch, cudaStream_t st
     if (key_in_output) nblk_main = min(nblk_main, (uint32_t)((key_off - out_off) / 16));
     const uint32_t nblk = (nbytes + 15) / 16;
     if (nblk_main > 0) {
-        dim3 grid((nblk_main + AES_BLOCKS_PER_CTA - 1) / AES_BLOCKS_PER_CTA, (unsigned)batch);
-        aes_ctr_kernel<<<grid, AES_THREADS, 256 * 32 * 4, st>>>(pool, pitch, key_off, out_off, nblk_main);
+        if (!set_smem_attr(aes_ctr_kernel, AES_SMEM)) return ST_CUDA;
+        // near-equal chunks of at most AES_BLOCKS_PER_CTA blocks per instance
+        const uint32_t chunks = (nblk_main + AES_BLOCKS_PER_CTA - 1) / AES_BLOCKS_PER_CTA;
+        const uint32_t bpc = (nblk_main + chunks - 1) / chunks;
+        dim3 grid(chunks, (unsigned)batch);
+        aes_ctr_kernel<<<grid, AES_THREADS, AES_SMEM, st>>>(pool, pitch, key_off, out_off, nblk_main, bpc, 128u);
     }
     if (nblk_main < nblk)
-        aes_ctr_tail_kernel<<<(unsigned)((batch + 127) / 128), 128, 0, st>>>(pool, pitch, key_off, out_off, nblk_main,
-                                                                               nbytes, (uint32_t)batch);
+        aes_ctr_tail_kernel<<<(unsigned)((batch + AES_TAIL_THREADS - 1) / AES_TAIL_THREADS), AES_TAIL_THREADS, 0, st>>>(
+            pool, pitch, key_off, out_off, nblk_main, nbytes, (uint32_t)batch);
     return cudaPeekAtLastError() == cudaSuccess ? ST_OK : ST_CUDA;
 }
 
