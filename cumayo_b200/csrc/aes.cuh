@@ -88,34 +88,55 @@ __device__ inline void aes128_key_schedule(const uint8_t *key, uint32_t *rk, con
     }
 }
 
-// Encrypt counter block `blk`; T points at the replicated table with this lane's column
-// already added (T + lane); rk in registers or shared.  Returns the 4 big-endian state words.
+// The four big-endian state words of an encrypted counter block.
 struct AesOut {
     uint32_t w0, w1, w2, w3;
 };
-template <class RK>
-__device__ __forceinline__ AesOut aes128_ctr_block(const uint32_t *T, const RK &rk, uint32_t blk) {
-#define TL(x) T[(x) << 5]
+
+// The table stride (128 bytes) as a value the compiler cannot fold, for kernels without a
+// launch argument for it (see aes128_ctr_block3): a constant-bank operand keeps the address
+// arithmetic an IMAD.
+__constant__ uint32_t c_aes_stride = 128;
+
+// Encrypt counter block `blk` with NTAB replicated tables addressed by IMAD: T0 at `base` (the
+// shared-memory address with this lane's column added) and, with NTAB = 2, ror16(T0) 32 KB above
+// it; the other round tables by PRMT rotations.  The work-queue kernel's form, whose CTA keeps
+// the tables where its P3 engine works later (two tables where that area holds them).
+template <int NTAB, class RK>
+__device__ __forceinline__ AesOut aes128_ctr_block1(uint32_t base, const RK &rk, uint32_t blk, uint32_t k128) {
+    static_assert(NTAB == 1 || NTAB == 2, "one or two tables");
+    auto t0 = [&](uint32_t x) {
+        uint32_t v;
+        asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(x * k128 + base));
+        return v;
+    };
+    auto t2 = [&](uint32_t x) {  // ror16(T0[x])
+        uint32_t v;
+        if constexpr (NTAB == 2)
+            asm volatile("ld.shared.u32 %0, [%1+32768];" : "=r"(v) : "r"(x * k128 + base));
+        else
+            v = ror16(t0(x));
+        return v;
+    };
     uint32_t s0 = rk[0], s1 = rk[1], s2 = rk[2], s3 = blk ^ rk[3];
 #pragma unroll
     for (int r = 1; r < 10; r++) {
-        uint32_t t0 = TL(s0 >> 24) ^ ror8(TL(byte_of(s1, 2))) ^ ror16(TL(byte_of(s2, 1))) ^ ror24(TL(byte_of(s3, 0))) ^
-                      rk[4 * r];
-        uint32_t t1 = TL(s1 >> 24) ^ ror8(TL(byte_of(s2, 2))) ^ ror16(TL(byte_of(s3, 1))) ^ ror24(TL(byte_of(s0, 0))) ^
-                      rk[4 * r + 1];
-        uint32_t t2 = TL(s2 >> 24) ^ ror8(TL(byte_of(s3, 2))) ^ ror16(TL(byte_of(s0, 1))) ^ ror24(TL(byte_of(s1, 0))) ^
-                      rk[4 * r + 2];
-        uint32_t t3 = TL(s3 >> 24) ^ ror8(TL(byte_of(s0, 2))) ^ ror16(TL(byte_of(s1, 1))) ^ ror24(TL(byte_of(s2, 0))) ^
-                      rk[4 * r + 3];
-        s0 = t0;
-        s1 = t1;
-        s2 = t2;
-        s3 = t3;
+        const uint32_t a = t0(s0 >> 24) ^ ror8(t0(byte_of(s1, 2))) ^ t2(byte_of(s2, 1)) ^ ror8(t2(byte_of(s3, 0))) ^
+                           rk[4 * r];
+        const uint32_t b = t0(s1 >> 24) ^ ror8(t0(byte_of(s2, 2))) ^ t2(byte_of(s3, 1)) ^ ror8(t2(byte_of(s0, 0))) ^
+                           rk[4 * r + 1];
+        const uint32_t c = t0(s2 >> 24) ^ ror8(t0(byte_of(s3, 2))) ^ t2(byte_of(s0, 1)) ^ ror8(t2(byte_of(s1, 0))) ^
+                           rk[4 * r + 2];
+        const uint32_t d = t0(s3 >> 24) ^ ror8(t0(byte_of(s0, 2))) ^ t2(byte_of(s1, 1)) ^ ror8(t2(byte_of(s2, 0))) ^
+                           rk[4 * r + 3];
+        s0 = a;
+        s1 = b;
+        s2 = c;
+        s3 = d;
     }
-    // last round: S-box = byte 1 of T0[x]; gather four S-box bytes per output word with PRMT
 #define LASTW(a, b, c, d, k)                                                                   \
-    (__byte_perm(__byte_perm(TL((a) >> 24), TL(byte_of(b, 2)), 0x1500),                         \
-                 __byte_perm(TL(byte_of(c, 1)), TL(byte_of(d, 0)), 0x0015), 0x3254) ^            \
+    (__byte_perm(__byte_perm(t0((a) >> 24), t0(byte_of(b, 2)), 0x1500),                         \
+                 __byte_perm(t0(byte_of(c, 1)), t0(byte_of(d, 0)), 0x0015), 0x3254) ^            \
      rk[k])
     AesOut o;
     o.w0 = LASTW(s0, s1, s2, s3, 40);
@@ -123,7 +144,6 @@ __device__ __forceinline__ AesOut aes128_ctr_block(const uint32_t *T, const RK &
     o.w2 = LASTW(s2, s3, s0, s1, 42);
     o.w3 = LASTW(s3, s0, s1, s2, 43);
 #undef LASTW
-#undef TL
     return o;
 }
 

@@ -46,7 +46,10 @@ struct QueueCfg<SET, MAYO_B200_OP_KEYPAIR> {
     using S = Set<SET>;
     using KC = KeyCfg<SET>;
     static constexpr int NT = KC::NT;
-    static constexpr size_t aes_end = 256 * 32 * 4 + 44 * 4;  // replicated T0 + round keys
+    // replicated T0 (and ror16(T0) where the P3 engine's area below O holds both: MAYO_5) and the
+    // round keys; the tables are dead once the keystream is written
+    static constexpr int NTAB = KC::off_o >= 2 * 256 * 32 * 4 + 44 * 4 ? 2 : 1;
+    static constexpr size_t aes_end = NTAB * 256 * 32 * 4 + 44 * 4;
     static_assert(KC::off_o >= aes_end, "O must not overlap the AES tables");
     static constexpr size_t seedpk = KC::off_o + pad16(S::o_bytes);
     static constexpr size_t smem = seedpk + 16;
@@ -208,19 +211,25 @@ __device__ void queue_keypair(uint8_t *smem, int tid, const QueueOps &ops, uint3
     }
     __syncthreads();
     // AES-CTR of P1 || P2 into this CTA's scratch (src/keypair.cu:52)
+    constexpr int NTAB = QueueCfg<SET, MAYO_B200_OP_KEYPAIR>::NTAB;
     uint32_t *T = reinterpret_cast<uint32_t *>(smem);
-    uint32_t *rk_s = T + 256 * 32;
-    for (int i = tid; i < 256 * 32; i += NT) T[i] = c_aes.te0[i >> 5];
+    uint32_t *rk_s = T + NTAB * 256 * 32;
+    for (int i = tid; i < 256 * 32; i += NT) {
+        const uint32_t v = c_aes.te0[i >> 5];
+        T[i] = v;
+        if (NTAB == 2) T[256 * 32 + i] = ror16(v);
+    }
     if (tid == 0) aes128_key_schedule(s_seedpk, rk_s);
     __syncthreads();
     {
         uint32_t rk[44];
 #pragma unroll
         for (int i = 0; i < 44; i++) rk[i] = rk_s[i];
-        const uint32_t *Tl = T + (tid & 31);
+        const uint32_t base = (uint32_t)__cvta_generic_to_shared(T + (tid & 31));
+        const uint32_t k128 = c_aes_stride;
         const uint32_t nblk = (S::p + 15) / 16;  // the scratch has room for the whole last block
         for (uint32_t blk = tid; blk < nblk; blk += NT) {
-            const AesOut o = aes128_ctr_block(Tl, rk, blk);
+            const AesOut o = aes128_ctr_block1<NTAB>(base, rk, blk, k128);
             st16(scratch + (size_t)blk * 16, bswap32(o.w0), bswap32(o.w1), bswap32(o.w2), bswap32(o.w3));
         }
     }
