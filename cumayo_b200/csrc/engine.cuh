@@ -182,6 +182,26 @@ struct Engine {
         }
     }
 
+    // Ask L2 for the entries of rows [r0, r0 + R) (those < nrows), both 128-byte lines an entry
+    // can touch, one warp issuing (lane = 0..31); no completion to wait for.  Called one pass
+    // ahead of convert, so that the next rows' loads hit L2 instead of HBM.
+    template <class Rows>
+    __device__ __forceinline__ void prefetch(const Rows &rows, int r0, int nrows, int lane) const {
+#pragma unroll 1
+        for (int slot = 0; slot < R; slot++) {
+            const int r = r0 + slot;
+            if (r >= nrows) break;
+            const int cnt = rows.count(r);
+            for (int e = lane; e < cnt; e += 32) {
+                const uint8_t *p = rows.entry(r, e);
+                if (p) {
+                    asm volatile("prefetch.L2 [%0];" ::"l"(p));
+                    asm volatile("prefetch.L2 [%0];" ::"l"(p + S::menc - 1));
+                }
+            }
+        }
+    }
+
     // T_j[r] for this thread's (j, w) over row r = r0 + rs (call only when active and r < nrows).
     template <class Rows>
     __device__ __forceinline__ G4 row_product(const Rows &rows, int r) const {

@@ -93,6 +93,8 @@ __device__ __forceinline__ void p3_instance(uint8_t *smem, int tid, const uint8_
     for (int i = 0; i < J; i++) X[i] = g4_zero();
 #pragma unroll 1
     for (int r0 = 0; r0 < S::v; r0 += R) {
+        // the next pass's rows into L2 (MAYO_1/3/5 keypairs 1-5 % faster, MAYO_2's 4 % slower)
+        if (SET != 2 && tid < 32) eng.prefetch(rows, r0 + R, S::v, tid);
         eng.convert(rows, r0, S::v, tid, NT);
         __syncthreads();
         const int r = r0 + eng.rs;

@@ -106,6 +106,7 @@ __global__ void __launch_bounds__(KeyCfg<SET>::NT) l_kernel(uint8_t *pool, size_
     const LRows<SET> rows{P1, P2};
 #pragma unroll 1
     for (int r0 = 0; r0 < S::v; r0 += R) {
+        if (SET >= 3 && tid < 32) eng.prefetch(rows, r0 + R, S::v, tid);  // next pass into L2
         eng.convert(rows, r0, S::v, tid, NT);
         __syncthreads();
         const int r = r0 + eng.rs;

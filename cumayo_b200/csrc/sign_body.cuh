@@ -325,6 +325,14 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem0, int T, const uint8_
         const P1Rows<SET> rows{P1};
 #pragma unroll 1
         for (int r0 = 0; r0 < S::v; r0 += R) {
+            // the next pass's rows of P1, or after the last the first columns of L, into L2:
+            // MAYO_3/5 (MAYO_5 signWithesk 6.96 -> 6.63 ms per 1,024; MAYO_1/2 measured slower)
+            if (SET >= 3 && tid < 32) {
+                if (r0 + R < S::v)
+                    eng.prefetch(rows, r0 + R, S::v, tid);
+                else
+                    eng.prefetch(LColRows<SET>{L}, 0, S::o, tid);
+            }
             eng.convert(rows, r0, S::v, tid, NT);
             __syncthreads();
             const int r = r0 + eng.rs;
@@ -392,6 +400,7 @@ __device__ __forceinline__ bool sign_attempt(uint8_t *smem0, int T, const uint8_
         const LColRows<SET> rows{L};
 #pragma unroll 1
         for (int b0 = 0; b0 < S::o; b0 += R) {
+            if (SET >= 3 && tid < 32) eng.prefetch(rows, b0 + R, S::o, tid);
             eng.convert(rows, b0, S::o, tid, NT);
             __syncthreads();
             const int b = b0 + eng.rs;

@@ -120,6 +120,10 @@ __device__ __forceinline__ void verify_instance(uint8_t *smem, int tid, const ui
         } else {
 #pragma unroll 1
             for (int r0 = 0; r0 < S::n; r0 += R) {
+                // the next pass's key rows into L2 (measured: MAYO_5 distinct-key verify 0.745 ->
+                // 0.780 M/s, MAYO_1 verifyWithepk 1 % faster; MAYO_2's 3 % slower, and MAYO_3's
+                // kernel, held to 80 registers, spills with it)
+                if ((SET == 1 || SET == 5) && tid < 32) eng.prefetch(rows, r0 + R, S::n, tid);
                 eng.convert(rows, r0, S::n, tid, NC);
                 bar_sync(1, NC);
                 const int r = r0 + eng.rs;
