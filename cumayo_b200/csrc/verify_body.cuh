@@ -52,6 +52,25 @@ struct VerifyRows {
         return P3 + (size_t)tri(rr, rr + e, S::o) * S::menc;
     }
     __device__ __forceinline__ int col(int r, int e) const { return r + e; }
+    // Ask L2 for row r's entries, one warp issuing (lane = 0..31): rows of P1 || P2 and of P3 are
+    // contiguous runs of m-vectors, so one prefetch per 128-byte line of each run.
+    __device__ __forceinline__ void prefetch(int r, int lane) const {
+        if (r < S::v) {
+            prefetch_lines(P1 + (size_t)tri(r, r, S::v) * S::menc, (S::v - r) * S::menc, lane);
+            prefetch_lines(P2 + (size_t)r * S::o * S::menc, S::o * S::menc, lane);
+        } else if (r < S::n) {
+            const int rr = r - S::v;
+            prefetch_lines(P3 + (size_t)tri(rr, rr, S::o) * S::menc, (S::o - rr) * S::menc, lane);
+        }
+    }
+    // every address issued lies in [p, p + n): the first is p, the others start 128-byte lines
+    __device__ __forceinline__ static void prefetch_lines(const uint8_t *p, int n, int lane) {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(p), end = a + (uintptr_t)n;
+        for (uintptr_t l = (a & ~uintptr_t(127)) + 128u * (uintptr_t)lane; l < end; l += 128u * 32u) {
+            const uintptr_t q = l < a ? a : l;
+            asm volatile("prefetch.L2 [%0];" ::"l"(q));
+        }
+    }
 };
 
 __device__ __forceinline__ int pair_index(int i, int j, int k) { return i * k - (i * (i - 1)) / 2 + (j - i); }
@@ -120,10 +139,16 @@ __device__ __forceinline__ void verify_instance(uint8_t *smem, int tid, const ui
         } else {
 #pragma unroll 1
             for (int r0 = 0; r0 < S::n; r0 += R) {
-                // the next pass's key rows into L2 (measured: MAYO_5 distinct-key verify 0.745 ->
-                // 0.780 M/s, MAYO_1 verifyWithepk 1 % faster; MAYO_2's 3 % slower, and MAYO_3's
-                // kernel, held to 80 registers, spills with it)
-                if ((SET == 1 || SET == 5) && tid < 32) eng.prefetch(rows, r0 + R, S::n, tid);
+                // the next pass's key rows into L2, per entry (MAYO_1/5: distinct-key verify of
+                // MAYO_5 0.745 -> 0.780 M/s, MAYO_1 verifyWithepk 1 % faster) or per 128-byte line of
+                // each row's runs (MAYO_3, whose kernel is held to 80 registers: verifyWithepk 3 %
+                // faster); MAYO_2's measured 3 % slower with either
+                if (tid < 32) {
+                    if constexpr (SET == 1 || SET == 5) eng.prefetch(rows, r0 + R, S::n, tid);
+                    if constexpr (SET == 3)
+#pragma unroll 1
+                        for (int q = 0; q < R; q++) rows.prefetch(r0 + R + q, tid);
+                }
                 eng.convert(rows, r0, S::n, tid, NC);
                 bar_sync(1, NC);
                 const int r = r0 + eng.rs;
