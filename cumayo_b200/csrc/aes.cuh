@@ -12,6 +12,8 @@
 // compile time from GF(2^8) arithmetic.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace mayo {
@@ -94,102 +96,68 @@ struct AesOut {
 };
 
 // The table stride (128 bytes) as a value the compiler cannot fold, for kernels without a
-// launch argument for it (see aes128_ctr_block3): a constant-bank operand keeps the address
-// arithmetic an IMAD.
+// launch argument for it: a constant-bank operand keeps the address arithmetic an IMAD.
 __constant__ uint32_t c_aes_stride = 128;
 
-// Encrypt counter block `blk` with NTAB replicated tables addressed by IMAD: T0 at `base` (the
-// shared-memory address with this lane's column added) and, with NTAB = 2, ror16(T0) 32 KB above
-// it; the other round tables by PRMT rotations.  The work-queue kernel's form, whose CTA keeps
-// the tables where its P3 engine works later (two tables where that area holds them).
+// Encrypt counter block `blk` with NTAB replicated round tables in shared memory, 32 KB apart
+// from `base` (the shared-memory address of T0 with this lane's column added):
+//   NTAB = 3: T0, ror8(T0), ror16(T0)   (the expansion kernel, 96 KB)
+//   NTAB = 2: T0, ror16(T0)             (the work queue's keypair where its P3 area holds both)
+//   NTAB = 1: T0                        (the work queue's keypair otherwise)
+// the other round tables by PRMT rotations.  A lookup is a byte extraction, one IMAD for the
+// address (the multiplier `k128` = 128 is a kernel argument or a constant-bank value, so the
+// address arithmetic stays on the IMAD pipe instead of joining the extractions, rotations and
+// XORs on the logic pipe, which with the table reads sets the pace) and the read.  Measured at
+// MAYO_1's 1,024 x 9,031 blocks: one table with PRMT rotations and shifted-index addresses
+// 0.250 ms, IMAD addresses 0.234, two tables 0.222, three tables in two CTAs of 384 threads per
+// SM 0.203 (byte-exact).
 template <int NTAB, class RK>
-__device__ __forceinline__ AesOut aes128_ctr_block1(uint32_t base, const RK &rk, uint32_t blk, uint32_t k128) {
-    static_assert(NTAB == 1 || NTAB == 2, "one or two tables");
-    auto t0 = [&](uint32_t x) {
+__device__ __forceinline__ AesOut aes128_ctr_block_t(uint32_t base, const RK &rk, uint32_t blk, uint32_t k128) {
+    static_assert(NTAB >= 1 && NTAB <= 3, "one to three tables");
+    auto ld = [&](uint32_t x, auto tab) {
+        constexpr int T = decltype(tab)::value;
         uint32_t v;
-        asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(x * k128 + base));
-        return v;
-    };
-    auto t2 = [&](uint32_t x) {  // ror16(T0[x])
-        uint32_t v;
-        if constexpr (NTAB == 2)
+        if constexpr (T == 0)
+            asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(x * k128 + base));
+        else if constexpr (T == 1)
             asm volatile("ld.shared.u32 %0, [%1+32768];" : "=r"(v) : "r"(x * k128 + base));
         else
-            v = ror16(t0(x));
+            asm volatile("ld.shared.u32 %0, [%1+65536];" : "=r"(v) : "r"(x * k128 + base));
         return v;
+    };
+    using I0 = std::integral_constant<int, 0>;
+    using I1 = std::integral_constant<int, 1>;
+    using I2 = std::integral_constant<int, 2>;
+    auto r0 = [&](uint32_t x) { return ld(x, I0{}); };  // T0[x]
+    auto r8 = [&](uint32_t x) {                          // ror8(T0[x])
+        if constexpr (NTAB == 3) return ld(x, I1{});
+        else return ror8(ld(x, I0{}));
+    };
+    auto r16 = [&](uint32_t x) {  // ror16(T0[x])
+        if constexpr (NTAB == 3) return ld(x, I2{});
+        else if constexpr (NTAB == 2) return ld(x, I1{});
+        else return ror16(ld(x, I0{}));
+    };
+    auto r24 = [&](uint32_t x) {  // ror24(T0[x])
+        if constexpr (NTAB == 1) return ror24(ld(x, I0{}));
+        else return ror8(r16(x));
     };
     uint32_t s0 = rk[0], s1 = rk[1], s2 = rk[2], s3 = blk ^ rk[3];
 #pragma unroll
     for (int r = 1; r < 10; r++) {
-        const uint32_t a = t0(s0 >> 24) ^ ror8(t0(byte_of(s1, 2))) ^ t2(byte_of(s2, 1)) ^ ror8(t2(byte_of(s3, 0))) ^
-                           rk[4 * r];
-        const uint32_t b = t0(s1 >> 24) ^ ror8(t0(byte_of(s2, 2))) ^ t2(byte_of(s3, 1)) ^ ror8(t2(byte_of(s0, 0))) ^
-                           rk[4 * r + 1];
-        const uint32_t c = t0(s2 >> 24) ^ ror8(t0(byte_of(s3, 2))) ^ t2(byte_of(s0, 1)) ^ ror8(t2(byte_of(s1, 0))) ^
-                           rk[4 * r + 2];
-        const uint32_t d = t0(s3 >> 24) ^ ror8(t0(byte_of(s0, 2))) ^ t2(byte_of(s1, 1)) ^ ror8(t2(byte_of(s2, 0))) ^
-                           rk[4 * r + 3];
+        const uint32_t a = r0(s0 >> 24) ^ r8(byte_of(s1, 2)) ^ r16(byte_of(s2, 1)) ^ r24(byte_of(s3, 0)) ^ rk[4 * r];
+        const uint32_t b = r0(s1 >> 24) ^ r8(byte_of(s2, 2)) ^ r16(byte_of(s3, 1)) ^ r24(byte_of(s0, 0)) ^ rk[4 * r + 1];
+        const uint32_t c = r0(s2 >> 24) ^ r8(byte_of(s3, 2)) ^ r16(byte_of(s0, 1)) ^ r24(byte_of(s1, 0)) ^ rk[4 * r + 2];
+        const uint32_t d = r0(s3 >> 24) ^ r8(byte_of(s0, 2)) ^ r16(byte_of(s1, 1)) ^ r24(byte_of(s2, 0)) ^ rk[4 * r + 3];
         s0 = a;
         s1 = b;
         s2 = c;
         s3 = d;
     }
-#define LASTW(a, b, c, d, k)                                                                   \
-    (__byte_perm(__byte_perm(t0((a) >> 24), t0(byte_of(b, 2)), 0x1500),                         \
-                 __byte_perm(t0(byte_of(c, 1)), t0(byte_of(d, 0)), 0x0015), 0x3254) ^            \
-     rk[k])
-    AesOut o;
-    o.w0 = LASTW(s0, s1, s2, s3, 40);
-    o.w1 = LASTW(s1, s2, s3, s0, 41);
-    o.w2 = LASTW(s2, s3, s0, s1, 42);
-    o.w3 = LASTW(s3, s0, s1, s2, 43);
-#undef LASTW
-    return o;
-}
-
-// The same block with three replicated tables in shared memory: T0, ror8(T0) and ror16(T0) at
-// byte offsets 0, 32 KB and 64 KB from `base` (this lane's column already added), the fourth
-// table as ror8 of the third.  A lookup is a byte extraction, one IMAD for the address and the
-// read; the multiplier `k128` (= 128, the table stride) is a kernel argument so that the address
-// arithmetic stays on the IMAD pipe instead of joining the extractions, rotations and XORs on the
-// logic pipe, which with the table reads sets the pace (measured at MAYO_1's 1,024 x 9,031
-// blocks: one table with PRMT rotations 0.250 ms, three tables 0.203 ms, byte-exact).
-template <class RK>
-__device__ __forceinline__ AesOut aes128_ctr_block3(uint32_t base, const RK &rk, uint32_t blk, uint32_t k128) {
-    auto t0 = [&](uint32_t x) {
-        uint32_t v;
-        asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(x * k128 + base));
-        return v;
-    };
-    auto t1 = [&](uint32_t x) {
-        uint32_t v;
-        asm volatile("ld.shared.u32 %0, [%1+32768];" : "=r"(v) : "r"(x * k128 + base));
-        return v;
-    };
-    auto t2 = [&](uint32_t x) {
-        uint32_t v;
-        asm volatile("ld.shared.u32 %0, [%1+65536];" : "=r"(v) : "r"(x * k128 + base));
-        return v;
-    };
-    uint32_t s0 = rk[0], s1 = rk[1], s2 = rk[2], s3 = blk ^ rk[3];
-#pragma unroll
-    for (int r = 1; r < 10; r++) {
-        const uint32_t t0w = t0(s0 >> 24) ^ t1(byte_of(s1, 2)) ^ t2(byte_of(s2, 1)) ^ ror8(t2(byte_of(s3, 0))) ^ rk[4 * r];
-        const uint32_t t1w =
-            t0(s1 >> 24) ^ t1(byte_of(s2, 2)) ^ t2(byte_of(s3, 1)) ^ ror8(t2(byte_of(s0, 0))) ^ rk[4 * r + 1];
-        const uint32_t t2w =
-            t0(s2 >> 24) ^ t1(byte_of(s3, 2)) ^ t2(byte_of(s0, 1)) ^ ror8(t2(byte_of(s1, 0))) ^ rk[4 * r + 2];
-        const uint32_t t3w =
-            t0(s3 >> 24) ^ t1(byte_of(s0, 2)) ^ t2(byte_of(s1, 1)) ^ ror8(t2(byte_of(s2, 0))) ^ rk[4 * r + 3];
-        s0 = t0w;
-        s1 = t1w;
-        s2 = t2w;
-        s3 = t3w;
-    }
     // last round: S-box = byte 1 of T0[x]
 #define LASTW(a, b, c, d, k)                                                                   \
-    (__byte_perm(__byte_perm(t0((a) >> 24), t0(byte_of(b, 2)), 0x1500),                         \
-                 __byte_perm(t0(byte_of(c, 1)), t0(byte_of(d, 0)), 0x0015), 0x3254) ^            \
+    (__byte_perm(__byte_perm(r0((a) >> 24), r0(byte_of(b, 2)), 0x1500),                         \
+                 __byte_perm(r0(byte_of(c, 1)), r0(byte_of(d, 0)), 0x0015), 0x3254) ^            \
      rk[k])
     AesOut o;
     o.w0 = LASTW(s0, s1, s2, s3, 40);
@@ -242,13 +210,15 @@ static __global__ void __launch_bounds__(AES_THREADS, 2)
     extern __shared__ uint32_t aes_smem[];  // [3][256 * 32] words
     __shared__ uint32_t rk_s[44];
     uint8_t *row = pool + (size_t)blockIdx.y * pitch;
-    for (int i = threadIdx.x; i < 256 * 32; i += AES_THREADS) {
+    // warp 0's lane 0 runs the (serial) key schedule while the other warps build the tables
+    if (threadIdx.x == 0) aes128_key_schedule(row + key_off, rk_s);
+    for (int i = (int)threadIdx.x - 32; i < 256 * 32; i += AES_THREADS - 32) {
+        if (i < 0) break;
         const uint32_t v = c_aes.te0[i >> 5];
         aes_smem[i] = v;
         aes_smem[256 * 32 + i] = ror8(v);
         aes_smem[2 * 256 * 32 + i] = ror16(v);
     }
-    if (threadIdx.x == 0) aes128_key_schedule(row + key_off, rk_s);
     __syncthreads();
     uint32_t rk[44];
 #pragma unroll
@@ -258,7 +228,7 @@ static __global__ void __launch_bounds__(AES_THREADS, 2)
     const uint32_t b0 = blockIdx.x * bpc;
     const uint32_t b1 = min(b0 + bpc, nblk_main);
     for (uint32_t blk = b0 + threadIdx.x; blk < b1; blk += AES_THREADS) {
-        AesOut o = aes128_ctr_block3(base, rk, blk, k128);
+        AesOut o = aes128_ctr_block_t<3>(base, rk, blk, k128);
         st16(out + (size_t)blk * 16, bswap32(o.w0), bswap32(o.w1), bswap32(o.w2), bswap32(o.w3));
     }
 }

@@ -229,7 +229,7 @@ __device__ void queue_keypair(uint8_t *smem, int tid, const QueueOps &ops, uint3
         const uint32_t k128 = c_aes_stride;
         const uint32_t nblk = (S::p + 15) / 16;  // the scratch has room for the whole last block
         for (uint32_t blk = tid; blk < nblk; blk += NT) {
-            const AesOut o = aes128_ctr_block1<NTAB>(base, rk, blk, k128);
+            const AesOut o = aes128_ctr_block_t<NTAB>(base, rk, blk, k128);
             st16(scratch + (size_t)blk * 16, bswap32(o.w0), bswap32(o.w1), bswap32(o.w2), bswap32(o.w3));
         }
     }
