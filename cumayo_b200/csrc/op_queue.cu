@@ -214,12 +214,14 @@ __device__ void queue_keypair(uint8_t *smem, int tid, const QueueOps &ops, uint3
     constexpr int NTAB = QueueCfg<SET, MAYO_B200_OP_KEYPAIR>::NTAB;
     uint32_t *T = reinterpret_cast<uint32_t *>(smem);
     uint32_t *rk_s = T + NTAB * 256 * 32;
-    for (int i = tid; i < 256 * 32; i += NT) {
+    // warp 0's lane 0 runs the (serial) key schedule while the other warps build the tables
+    if (tid == 0) aes128_key_schedule(s_seedpk, rk_s);
+    for (int i = tid - 32; i < 256 * 32; i += NT - 32) {
+        if (i < 0) break;
         const uint32_t v = c_aes.te0[i >> 5];
         T[i] = v;
         if (NTAB == 2) T[256 * 32 + i] = ror16(v);
     }
-    if (tid == 0) aes128_key_schedule(s_seedpk, rk_s);
     __syncthreads();
     {
         uint32_t rk[44];

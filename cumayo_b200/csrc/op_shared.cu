@@ -1042,7 +1042,8 @@ __global__ void __launch_bounds__(VTailCfg<SET>::NT)
         G4 X[J];
 #pragma unroll
         for (int i = 0; i < J; i++) X[i] = g4_zero();
-#pragma unroll 1
+        // unrolled so that several rows' plane loads are in flight at once
+#pragma unroll 2
         for (int r = rs; r < S::n; r += R) {
             const G4 T = g4_ld(pl + (size_t)r * W);
             const uint4 *mr = masks + (size_t)r * J;
