@@ -7,9 +7,9 @@
 // shared memory, entry x of copy c at word 32*x + c, so lane c always hits bank c and the 16
 // data-dependent lookups of a round never conflict.  The other three round tables are byte
 // rotations of T0.  The expansion kernel keeps T0, ror8(T0) and ror16(T0) (96 KB, two CTAs of 384
-// threads per SM) and rotates only for the fourth; the work-queue kernel keeps T0 alone (32 KB)
-// and rotates with PRMT.  The S-box for the last round is byte 1 of T0[x].  Tables are computed at
-// compile time from GF(2^8) arithmetic.
+// threads per SM) and rotates only for the fourth; the work-queue kernel's keypair keeps T0 (and
+// ror16(T0) for MAYO_5) in the area its P3 engine uses next and rotates with PRMT.  The S-box for
+// the last round is byte 1 of T0[x].  Tables are computed at compile time from GF(2^8) arithmetic.
 #pragma once
 
 #include <type_traits>
