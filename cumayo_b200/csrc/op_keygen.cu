@@ -132,8 +132,12 @@ static int aes_expand(uint8_t *pool, size_t pitch, size_t batch, cudaStream_t st
         // near-equal chunks of at most AES_BLOCKS_PER_CTA blocks per instance
         const uint32_t chunks = (nblk_main + AES_BLOCKS_PER_CTA - 1) / AES_BLOCKS_PER_CTA;
         const uint32_t bpc = (nblk_main + chunks - 1) / chunks;
-        dim3 grid(chunks, (unsigned)batch);
-        aes_ctr_kernel<<<grid, AES_THREADS, AES_SMEM, st>>>(pool, pitch, key_off, out_off, nblk_main, bpc, 128u);
+        // instances on the grid's y dimension, at most 65,535 per launch
+        for (size_t b0 = 0; b0 < batch; b0 += 65535) {
+            const unsigned nb = (unsigned)(batch - b0 < 65535 ? batch - b0 : 65535);
+            aes_ctr_kernel<<<dim3(chunks, nb), AES_THREADS, AES_SMEM, st>>>(pool + b0 * pitch, pitch, key_off, out_off,
+                                                                             nblk_main, bpc, 128u);
+        }
     }
     if (nblk_main < nblk)
         aes_ctr_tail_kernel<<<(unsigned)((batch + AES_TAIL_THREADS - 1) / AES_TAIL_THREADS), AES_TAIL_THREADS, 0, st>>>(
